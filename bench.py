@@ -1,0 +1,417 @@
+"""Benchmark: mask-implicit-GEMM sparse conv on B200 (one training step of the
+200k-voxel LiDAR-like submanifold 3x3x3 layer, C = K = 64, bf16 operands,
+fp32 accumulation: forward + backward-input + backward-weight).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+* ``value``: whole-job algorithmic TFLOP/s, 3 * 2 * P * C * K per step (P =
+  valid voxel pairs; padded MMA rows are not counted), inputs resident in HBM,
+  per-step CUDA events on the launching stream around the three C-ABI calls,
+  L2 flushed (256 MB write) between steps, max over ranks.
+* ``e2e``: the same metric through the public API with host buffers: per step
+  the pinned-host coordinates, features and upstream gradient are copied in,
+  the pair table is built on the GPU, the three ops run, and output, input
+  gradient and weight gradient are copied back.
+* ``cpu_baseline`` / ``--impl reference``: the reference's own CPU algorithm
+  for this path (numpy gather-GEMM-scatter, cumm/conv/main_real_spconv.py:309-403)
+  restated in oracle/conv_oracle.py, fp32, BLAS on all host cores.
+Multi-GPU: independent clouds per rank (weak scaling, no collective on the
+data path).
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "cumm-rocm_b200"))
+
+N_VOX, C, K, KV = 200_000, 64, 64, 27
+WORKLOAD = "subm3x3x3_lidar200k_c64k64_bf16_fwd_dgrad_wgrad"
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d["bf16_tflops"], d["hbm_gbs"], "measured"
+    return 1590.0, 6650.0, "fallback"
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sms, maxs, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                maxs.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sms)) if sms else None,
+                "sm_max_mhz": float(max(maxs)) if maxs else None,
+                "samples": len(sms), "reasons": sorted(reasons)}
+
+
+def cpu_reference_step(x, w, dy, pf, pb):
+    """fp32 numpy gather-GEMM-scatter fwd + dgrad + wgrad (the reference's CPU path)."""
+    from oracle import conv_oracle as co
+    out = co.fwd_gather_gemm_scatter(x, w, pf, np.float32)
+    din = co.dgrad_gather_gemm_scatter(dy, w, pb, np.float32)
+    dw = co.wgrad_gather_gemm_scatter(dy, x, pf, np.float32)
+    return out, din, dw
+
+
+def _cpu_data(seed):
+    from cumm import voxelgen as vg
+    from oracle import pairs_oracle as po
+    coords = vg.lidar_voxels(N_VOX, seed=seed)
+    pf, pb, m = po.subm_pairs(coords, vg.KITTI_SHAPE)
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((N_VOX, C)).astype(np.float32)
+    dy = rng.standard_normal((N_VOX, K)).astype(np.float32)
+    w = vg.kaiming_uniform(K, KV, C, seed)
+    return coords, pf, pb, m, x, dy, w
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    threads = os.cpu_count() or 1
+    coords, pf, pb, m, x, dy, w = _cpu_data(0)
+    P = int((pf >= 0).sum())
+    flops = 3 * 2.0 * P * C * K
+    for _ in range(args.warmup):
+        cpu_reference_step(x, w, dy, pf, pb)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cpu_reference_step(x, w, dy, pf, pb)
+        times.append(time.perf_counter() - t0)
+    t = float(np.mean(times))
+    v = flops / t / 1e12
+    line = {
+        "metric": "implicit-GEMM spconv TFLOP/s (% BF16 peak)", "value": v, "unit": "TFLOP/s",
+        "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "voxels": N_VOX, "pairs": P, "C": C, "K": K,
+                   "parallelism": "cpu"},
+        "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+                         "sample": "full 200k-voxel layer, fwd+dgrad+wgrad per step, numpy fp32 "
+                                   "gather-GEMM-scatter (oracle/conv_oracle.py)"},
+        "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_b200(args, rank, world, dist):
+    import torch
+
+    from cumm import _lib
+    from cumm import tensorview as tv
+    from cumm import voxelgen as vg
+    from cumm.conv.main import build_conv_params_c, get_all_conv_algo_desp
+    from cumm.spconv_ops import build_pair_table
+    from cumm.tensorview.gemm import ConvOpType, ConvParams
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _lib.load()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    seed = rank
+    coords_np = vg.lidar_voxels(N_VOX, seed=seed)
+    rng = np.random.default_rng(seed)
+    x_np = rng.standard_normal((N_VOX, C)).astype(np.float32)
+    dy_np = rng.standard_normal((N_VOX, K)).astype(np.float32)
+    w_np = vg.kaiming_uniform(K, KV, C, seed)
+    coords = torch.from_numpy(coords_np).to(dev)
+    x = torch.from_numpy(x_np).to(dev).bfloat16()
+    dy = torch.from_numpy(dy_np).to(dev).bfloat16()
+    w = torch.from_numpy(w_np).to(dev).bfloat16()
+    pt = build_pair_table(coords, vg.KITTI_SHAPE)
+    P = pt.pair_count()
+    flops_op = 2.0 * P * C * K
+
+    def desp_for(op, dt_w=tv.bfloat16):
+        for d in get_all_conv_algo_desp():
+            if (d.op_type == op and d.algo == "Tcgen05" and d.dtype_input == tv.bfloat16 and
+                    d.dtype_weight == dt_w and d.dtype_output == tv.bfloat16 and
+                    d.tile_shape[0] == 128):
+                return d
+        raise KeyError(op)
+
+    out = torch.empty((N_VOX, K), dtype=torch.bfloat16, device=dev)
+    din = torch.empty((N_VOX, C), dtype=torch.bfloat16, device=dev)
+    dw = torch.empty((K, KV, C), dtype=torch.float32, device=dev)
+    mask_out = torch.empty(((N_VOX + 127) // 128,), dtype=torch.int32, device=dev)
+
+    def make(op, pt_, x_, w_, out_, dy_, din_, dw_, mo_):
+        p = ConvParams(3, op)
+        p.conv_algo_desp = desp_for(op, tv.float32 if op == ConvOpType.kBackwardWeight else tv.bfloat16)
+        if op == ConvOpType.kForward:
+            p.input, p.weight, p.output = tv.Tensor(x_), tv.Tensor(w_), tv.Tensor(out_)
+            p.indices = tv.Tensor(pt_.pairs_fwd)
+            p.mask = tv.Tensor(pt_.masks_fwd[0], tv.uint32)
+            p.mask_output = tv.Tensor(mo_, tv.uint32)
+        elif op == ConvOpType.kBackwardInput:
+            p.input, p.weight, p.output = tv.Tensor(din_), tv.Tensor(w_), tv.Tensor(dy_)
+            p.indices = tv.Tensor(pt_.pairs_bwd)
+            p.mask = tv.Tensor(pt_.masks_fwd[0], tv.uint32)
+            p.reverse_mask = True
+        else:
+            p.input, p.weight, p.output = tv.Tensor(x_), tv.Tensor(dw_), tv.Tensor(dy_)
+            p.indices = tv.Tensor(pt_.pairs_fwd)
+            p.mask = tv.Tensor(mo_, tv.uint32)
+            p.mask_width = 128
+        p.mask_argsort = tv.Tensor(pt_.argsorts_fwd[0])
+        p.stream = sptr
+        cp, _ = build_conv_params_c(p)
+        need = ctypes.c_int64(0)
+        _lib.check(lib.sc_conv_workspace_size(ctypes.byref(cp), ctypes.byref(need)))
+        ws = torch.empty(max(need.value, 256), dtype=torch.uint8, device=dev)
+        cp.workspace, cp.workspace_bytes = ws.data_ptr(), ws.numel()
+        return cp, ws
+
+    ops = [make(op, pt, x, w, out, dy, din, dw, mask_out)
+           for op in (ConvOpType.kForward, ConvOpType.kBackwardInput, ConvOpType.kBackwardWeight)]
+    call = lib.sc_conv_implicit_gemm
+
+    def step():
+        for cp, _ in ops:
+            rc = call(ctypes.byref(cp))
+            if rc:
+                _lib.check(rc)
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    bits = _lib.device_error_bits(sptr)
+    if bits:
+        raise RuntimeError(f"device error word {bits} during warm-up")
+
+    n_ev = args.steps
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(n_ev)]
+    sampler = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    for s in range(n_ev):
+        flush.zero_()
+        e = evs[s]
+        e[0].record(stream)
+        for i, (cp, _) in enumerate(ops):
+            rc = call(ctypes.byref(cp))
+            if rc:
+                _lib.check(rc)
+            e[i + 1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if dist is not None:
+        dist.barrier()
+    per_op = np.array([[evs[s][i].elapsed_time(evs[s][i + 1]) for i in range(3)]
+                       for s in range(n_ev)])  # ms
+    ms_op = per_op.mean(0)
+    ms_step = float(per_op.sum(1).mean())
+    bits = _lib.device_error_bits(sptr)
+    if bits:
+        raise RuntimeError(f"device error word {bits} during timing")
+    ms_max = ms_step
+    if dist is not None:
+        t = torch.tensor([ms_step], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = 3 * flops_op * world / (ms_max * 1e-3) / 1e12
+
+    # ---------------------------------------------------------------- end to end (public API)
+    coords_h = torch.from_numpy(coords_np).pin_memory()
+    x_h = torch.from_numpy(x_np).bfloat16().pin_memory()
+    dy_h = torch.from_numpy(dy_np).bfloat16().pin_memory()
+    out_h = torch.empty((N_VOX, K), dtype=torch.bfloat16).pin_memory()
+    din_h = torch.empty((N_VOX, C), dtype=torch.bfloat16).pin_memory()
+    dw_h = torch.empty((K, KV, C), dtype=torch.float32).pin_memory()
+    from cumm.conv.main import ConvMainUnitTest
+    cmt = ConvMainUnitTest()
+
+    def e2e_step():
+        cd = coords_h.to(dev, non_blocking=True)
+        xd = x_h.to(dev, non_blocking=True)
+        dyd = dy_h.to(dev, non_blocking=True)
+        ptd = build_pair_table(cd, vg.KITTI_SHAPE)
+        outd = torch.empty((N_VOX, K), dtype=torch.bfloat16, device=dev)
+        dind = torch.empty((N_VOX, C), dtype=torch.bfloat16, device=dev)
+        dwd = torch.empty((K, KV, C), dtype=torch.float32, device=dev)
+        mod = torch.empty(((N_VOX + 127) // 128,), dtype=torch.int32, device=dev)
+        for op in (ConvOpType.kForward, ConvOpType.kBackwardInput, ConvOpType.kBackwardWeight):
+            p = ConvParams(3, op)
+            p.conv_algo_desp = desp_for(op, tv.float32 if op == ConvOpType.kBackwardWeight
+                                        else tv.bfloat16)
+            if op == ConvOpType.kForward:
+                p.input, p.weight, p.output = tv.Tensor(xd), tv.Tensor(w), tv.Tensor(outd)
+                p.indices = tv.Tensor(ptd.pairs_fwd)
+                p.mask = tv.Tensor(ptd.masks_fwd[0], tv.uint32)
+                p.mask_output = tv.Tensor(mod, tv.uint32)
+            elif op == ConvOpType.kBackwardInput:
+                p.input, p.weight, p.output = tv.Tensor(dind), tv.Tensor(w), tv.Tensor(dyd)
+                p.indices = tv.Tensor(ptd.pairs_bwd)
+                p.mask = tv.Tensor(ptd.masks_fwd[0], tv.uint32)
+                p.reverse_mask = True
+            else:
+                p.input, p.weight, p.output = tv.Tensor(xd), tv.Tensor(dwd), tv.Tensor(dyd)
+                p.indices = tv.Tensor(ptd.pairs_fwd)
+                p.mask = tv.Tensor(mod, tv.uint32)
+                p.mask_width = 128
+            p.mask_argsort = tv.Tensor(ptd.argsorts_fwd[0])
+            p.stream = sptr
+            cmt.implicit_gemm2(p)
+        out_h.copy_(outd, non_blocking=True)
+        din_h.copy_(dind, non_blocking=True)
+        dw_h.copy_(dwd, non_blocking=True)
+        torch.cuda.synchronize()
+
+    for _ in range(2):
+        e2e_step()
+    n_e2e = max(3, min(args.steps, 20))
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(n_e2e):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / n_e2e
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = 3 * flops_op * world / (e2e_ms * 1e-3) / 1e12
+    h2d = coords_h.numel() * 4 + x_h.numel() * 2 + dy_h.numel() * 2
+    d2h = out_h.numel() * 2 + din_h.numel() * 2 + dw_h.numel() * 4
+
+    # ---------------------------------------------------------------- roofline of the dominant kernel
+    names = ["conv_fwd_rowgather", "conv_dgrad_rowgather", "conv_wgrad"]
+    dom = int(np.argmax(ms_op))
+    peak_tf, peak_bw, peak_kind = _peaks()
+    achieved = flops_op / (ms_op[dom] * 1e-3) / 1e12
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(names[dom])
+    roofline = {"bound": "tensor", "kernel": names[dom], "achieved": achieved, "peak": peak_tf,
+                "unit": "TFLOP/s", "frac": achieved / peak_tf, "peak_kind": peak_kind,
+                "traffic": traffic}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        _, pf, pb, _, xc, dyc, wc = _cpu_data(0)
+        t0 = time.perf_counter()
+        cpu_reference_step(xc, wc, dyc, pf, pb)
+        tc = time.perf_counter() - t0
+        Pc = int((pf >= 0).sum())
+        cpu = {"value": 3 * 2.0 * Pc * C * K / tc / 1e12, "unit": "TFLOP/s",
+               "cores": os.cpu_count(), "kind": "port",
+               "sample": "one full step (fwd+dgrad+wgrad) of the same 200k-voxel layer, numpy "
+                         "fp32 gather-GEMM-scatter, BLAS on all host cores"}
+
+    if rank == 0:
+        line = {
+            "metric": "implicit-GEMM spconv TFLOP/s (% BF16 peak)", "value": value,
+            "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "voxels": N_VOX, "pairs": P, "C": C, "K": K,
+                       "kernel": "3x3x3 subm", "l2": "flushed (256 MB write) between steps",
+                       "parallelism": f"replicas{world}"},
+            "per_op_ms": {names[i]: float(ms_op[i]) for i in range(3)},
+            "per_op_tflops": {names[i]: flops_op / (ms_op[i] * 1e-3) / 1e12 for i in range(3)},
+            "pct_bf16_peak": value / world / peak_tf,
+            "roofline": roofline,
+            "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+            "cpu_baseline": cpu,
+            "gpu_launches": 5 * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1 and args.impl == "b200":
+        import datetime
+
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+    try:
+        if args.impl == "reference":
+            if rank == 0:
+                run_reference(args, rank, world)
+        else:
+            run_b200(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

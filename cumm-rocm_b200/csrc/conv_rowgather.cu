@@ -1,0 +1,608 @@
+// conv_rowgather.cu - mask-implicit-GEMM sparse convolution, forward and
+// backward-input, on sm_100a tensor cores.
+//
+// Semantics follow the reference conv kernel (cumm/conv/kernel.py:737-1090):
+//   * rows are visited in mask_argsort order; a 128-row tile's mask is the OR
+//     of its rows' masks AND mask_filter (kernel.py:844-866); backward-input
+//     reverses it with brev(kmask) >> (32 - kv) (kernel.py:883-889) and skips
+//     tiles whose mask is zero (kernel.py:875-882);
+//   * for every offset k set in the tile mask, row r gathers
+//     A[indices[k][sigma(r)]] (zero when the index is -1,
+//     cumm/conv/sparse_iters.py:318-356, 625-648) and multiplies with the
+//     weight slab of offset k (cumm/gemm/blockmma/mma.py:445-578);
+//   * the epilogue writes row r to output row sigma(r) (permuted store,
+//     cumm/gemm/out_iters.py:537-551) with act(alpha*acc + beta*src).
+// The reference accumulates mask_output words per tile_shape[0] rows; here the
+// compute tile is always 128 rows and the mask of each tile_shape[0]-row
+// sub-tile (32/64/128) gates its own rows, which keeps results identical to a
+// tile_shape[0]-row kernel even for masks inconsistent with the index table.
+//
+// B200 design (one persistent CTA per SM, 13 warps, warp-specialised):
+//   warps 0-3   epilogue: TMEM -> registers -> permuted row stores
+//   warps 4-7   producers: 16-byte cp.async gathers of A rows and B slabs into
+//               SWIZZLE_128B shared-memory stages (one 128-byte reduction chunk
+//               per stage), completion handed to the MMA warp by mbarrier
+//   warps 8-11  index loaders: mask / argsort / indices of the next tiles into
+//               a 3-deep shared-memory ring (hides the argsort->index latency)
+//   warp 12     TMEM allocator + single-thread tcgen05.mma issuer into a
+//               double-buffered fp32 TMEM accumulator (128 lanes x BN columns)
+// Every mbarrier wait is bounded (globaltimer) and raises a CTA abort flag
+// plus kErrWaitTimeout instead of spinning forever.
+#include "kernels.h"
+
+namespace scb {
+namespace {
+
+constexpr int kThreads = 416;
+constexpr int kIdxStages = 3;
+constexpr int kTileM = 128;
+
+struct Meta {
+  int nchunks;
+  int n_active;
+  uint32_t tilemask;
+  uint32_t pad;
+  uint32_t grp[4];
+  int k_list[32];
+};
+
+struct KParams {
+  ConvRowGatherArgs a;
+  int64_t num_tiles;
+  int cpo;            // chunks per offset (a_row_bytes >= 128), else 0
+  int opc;            // offsets packed per chunk (a_row_bytes < 128)
+  int upo;            // 16-byte units per packed offset segment
+  int stages;
+  uint32_t stage_bytes;
+  uint32_t b_off;
+  uint32_t idx_off;
+  uint32_t idx_buf_bytes;
+  uint32_t bar_off;
+  uint32_t tmem_cols;
+  uint32_t idesc;
+};
+
+__device__ __forceinline__ void flag_error(int *err, int bits) { atomicOr(err, bits); }
+
+// ------------------------------------------------------------------ epilogue helpers
+template <int n, typename TOut>
+__device__ __forceinline__ void load_src(const TOut *p, float *v) {
+  if constexpr (sizeof(TOut) == 4) {
+#pragma unroll
+  for (int i = 0; i < n; i += 4) {
+    const float4 q = *reinterpret_cast<const float4 *>(p + i);
+    v[i] = q.x; v[i + 1] = q.y; v[i + 2] = q.z; v[i + 3] = q.w;
+  }
+  } else {
+#pragma unroll
+  for (int i = 0; i < n; i += 8) {
+    const uint4 q = *reinterpret_cast<const uint4 *>(p + i);
+    const TOut *h = reinterpret_cast<const TOut *>(&q);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[i + j] = to_f32(h[j]);
+  }
+  }
+}
+
+template <int n, typename TOut>
+__device__ __forceinline__ void store_row(TOut *p, const float *v) {
+  if constexpr (sizeof(TOut) == 4) {
+#pragma unroll
+    for (int i = 0; i < n; i += 4)
+      *reinterpret_cast<float4 *>(p + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < n; i += 8) {
+      uint4 q;
+      TOut *h = reinterpret_cast<TOut *>(&q);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) h[j] = from_f32<TOut>(v[i + j]);
+      *reinterpret_cast<uint4 *>(p + i) = q;
+    }
+  }
+}
+
+// Applies the epilogue to `n` (16 or 32) consecutive columns starting at column
+// `col` of output row `orow` and stores them.
+template <int n, typename TOut>
+__device__ __forceinline__ void epilogue_cols(const KParams &P, float *acc, int64_t orow, int col) {
+  const EpiParams &e = P.a.epi;
+  float src[32];
+  const bool use_src = e.beta != 0.f && e.src != nullptr;
+  if (use_src) {
+    const TOut *s = reinterpret_cast<const TOut *>(e.src) + orow * e.src_ld + col;
+    load_src<n, TOut>(s, src);
+  }
+  if (e.mode == 1) {
+    float bias[32];
+    if (e.bias != nullptr) load_src<n, TOut>(reinterpret_cast<const TOut *>(e.bias) + col, bias);
+#pragma unroll
+    for (int i = 0; i < n; ++i) {
+      float sc = e.scale != nullptr ? __ldg(e.scale + col + i) : 1.f;
+      float v = sc * acc[i] + (e.bias != nullptr ? e.alpha * bias[i] : 0.f);
+      if (use_src) v = fmaf(e.beta, src[i], v);
+      acc[i] = apply_act(v, e.act_type, e.act_alpha);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < n; ++i) {
+      float v = e.alpha * acc[i];
+      if (use_src) v = fmaf(e.beta, src[i], v);
+      acc[i] = apply_act(v, e.act_type, e.act_alpha);
+    }
+  }
+  TOut *dst = reinterpret_cast<TOut *>(P.a.out) + orow * P.a.out_ld + col;
+  store_row<n, TOut>(dst, acc);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ------------------------------------------------------------------ kernel
+template <bool kF8, typename TOut, int kLag>
+__global__ void __maxnreg__(152)
+    conv_rowgather_kernel(const __grid_constant__ KParams P) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw_u32 = smem_u32(smem_raw);
+  const uint32_t pad = (1024u - (raw_u32 & 1023u)) & 1023u;
+  uint8_t *smem = smem_raw + pad;
+  const uint32_t smem_base = raw_u32 + pad;
+
+  const int S = P.stages;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + P.bar_off);
+  uint64_t *full_bar = bars;
+  uint64_t *empty_bar = bars + S;
+  uint64_t *idx_full = bars + 2 * S;
+  uint64_t *idx_empty = idx_full + kIdxStages;
+  uint64_t *acc_full = idx_empty + kIdxStages;
+  uint64_t *acc_empty = acc_full + 2;
+  uint64_t *drain_bar = acc_empty + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain_bar + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const ConvRowGatherArgs &A = P.a;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < S; ++i) {
+      mbar_init(&full_bar[i], 128);
+      mbar_init(&empty_bar[i], 1);
+    }
+    for (int i = 0; i < kIdxStages; ++i) {
+      mbar_init(&idx_full[i], 128);
+      mbar_init(&idx_empty[i], 129);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&acc_full[i], 1);
+      mbar_init(&acc_empty[i], 128);
+    }
+    mbar_init(drain_bar, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 12) {
+    tmem_alloc(tmem_slot, P.tmem_cols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp >= 8 && warp < 12) {
+    // ---------------------------------------------------------------- index loaders
+    const int r = threadIdx.x - 256;  // row inside the tile
+    const int lw = r >> 5;
+    int it = 0;
+    for (int64_t tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
+      const int b = it % kIdxStages;
+      const uint32_t ph = (it / kIdxStages) & 1;
+      if (!mbar_wait(&idx_empty[b], ph ^ 1, abort_flag)) {
+        flag_error(A.err, kErrWaitTimeout);
+        break;
+      }
+      uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
+      int *tab = reinterpret_cast<int *>(buf);
+      Meta *meta = reinterpret_cast<Meta *>(buf + A.kv * kTileM * 4);
+      const int64_t tile_m = tile / A.n_tiles;
+      const int n_tile = static_cast<int>(tile % A.n_tiles);
+      const int64_t row_g = tile_m * kTileM + r;
+      const bool valid = row_g < A.M;
+      int sig = valid ? (A.argsort ? __ldg(A.argsort + row_g) : static_cast<int>(row_g)) : -1;
+      if (valid && (sig < 0 || sig >= A.out_rows)) {
+        flag_error(A.err, kErrBadIndex);
+        sig = -1;
+      }
+      // every loader warp reduces all four 32-row groups itself (no cross-warp
+      // barrier, so an aborted warp can never strand the others)
+      uint32_t gq[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int64_t rr = tile_m * kTileM + q * 32 + lane;
+        uint32_t v = rr < A.M ? (A.mask ? __ldg(A.mask + rr) : 1u) : 0u;
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, s);
+        gq[q] = v;
+      }
+      const uint32_t g0 = gq[0], g1 = gq[1], g2 = gq[2], g3 = gq[3];
+      uint32_t tm = (g0 | g1 | g2 | g3) & A.mask_filter;
+      uint32_t sub;
+      if (A.tile_m_desp == 32) {
+        sub = lw == 0 ? g0 : lw == 1 ? g1 : lw == 2 ? g2 : g3;
+      } else if (A.tile_m_desp == 64) {
+        sub = lw < 2 ? (g0 | g1) : (g2 | g3);
+      } else {
+        sub = g0 | g1 | g2 | g3;
+      }
+      sub &= A.mask_filter;
+      if (A.is_fwd && A.mask_out != nullptr && n_tile == 0 && r == 0) {
+        const int nsub = kTileM / A.tile_m_desp;
+        for (int d = 0; d < nsub; ++d) {
+          const int64_t start = tile_m * kTileM + d * A.tile_m_desp;
+          if (start >= A.M) break;
+          uint32_t w;
+          if (nsub == 4) w = d == 0 ? g0 : d == 1 ? g1 : d == 2 ? g2 : g3;
+          else if (nsub == 2) w = d == 0 ? (g0 | g1) : (g2 | g3);
+          else w = g0 | g1 | g2 | g3;
+          A.mask_out[start / A.tile_m_desp] = w & A.mask_filter;
+        }
+      }
+      if (A.reverse) {
+        tm = __brev(tm) >> (32 - A.kv);
+        sub = __brev(sub) >> (32 - A.kv);
+      }
+      int vals[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        int v = -1;
+        if (k < A.kv && ((tm >> k) & 1u) && sig >= 0 && ((sub >> k) & 1u)) {
+          if (A.indices)
+            v = __ldg(A.indices + static_cast<int64_t>(k) * A.M + sig);
+          else
+            v = A.a_inds ? __ldg(A.a_inds + row_g) : static_cast<int>(row_g);
+        }
+        vals[k] = v;
+      }
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        if (k < A.kv && ((tm >> k) & 1u)) {
+          int v = vals[k];
+          if (v < -1 || v >= A.a_rows) {
+            flag_error(A.err, kErrBadIndex);
+            v = -1;
+          }
+          const int slot = __popc(tm & ((1u << k) - 1u));
+          tab[slot * kTileM + r] = v;
+        }
+      }
+      if (r == 0) {
+        const int na = __popc(tm);
+        int s = 0;
+        uint32_t mm = tm;
+        while (mm) {
+          const int k = __ffs(mm) - 1;
+          mm &= mm - 1;
+          meta->k_list[s++] = k;
+        }
+        meta->n_active = na;
+        meta->tilemask = tm;
+        meta->nchunks = P.cpo > 0 ? na * P.cpo : (na + P.opc - 1) / P.opc;
+      }
+      // the group words are re-read by nobody after this point; all writes of
+      // this thread are released by its arrive
+      mbar_arrive(&idx_full[b]);
+    }
+  } else if (warp >= 4 && warp < 8) {
+    // ---------------------------------------------------------------- producers
+    const int pt = threadIdx.x - 128;
+    const int u = pt & 7;
+    const int rg = pt >> 3;
+    int it = 0;
+    int64_t chunk_ctr = 0;
+    int outstanding = 0;
+    bool ok = true;
+    auto drain = [&]() {
+      cp_async_wait_all();
+      fence_proxy_async_smem();
+      while (outstanding > 0) {
+        const int64_t c = chunk_ctr - outstanding;
+        mbar_arrive(&full_bar[c % S]);
+        --outstanding;
+      }
+    };
+    for (int64_t tile = blockIdx.x; tile < P.num_tiles && ok; tile += gridDim.x, ++it) {
+      const int b = it % kIdxStages;
+      const uint32_t ph = (it / kIdxStages) & 1;
+      if (!mbar_try_wait(&idx_full[b], ph)) {
+        drain();
+        if (!mbar_wait(&idx_full[b], ph, abort_flag)) {
+          flag_error(A.err, kErrWaitTimeout);
+          break;
+        }
+      }
+      const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
+      const int *tab = reinterpret_cast<const int *>(buf);
+      const Meta *meta = reinterpret_cast<const Meta *>(buf + A.kv * kTileM * 4);
+      const int nch = meta->nchunks;
+      const int na = meta->n_active;
+      const int n0 = static_cast<int>(tile % A.n_tiles) * A.BN;
+      for (int j = 0; j < nch; ++j) {
+        const int s = static_cast<int>(chunk_ctr % S);
+        const uint32_t eph = static_cast<uint32_t>((chunk_ctr / S) & 1);
+        if (!mbar_wait(&empty_bar[s], eph ^ 1, abort_flag)) {
+          flag_error(A.err, kErrWaitTimeout);
+          ok = false;
+          break;
+        }
+        const uint32_t sA = smem_base + s * P.stage_bytes;
+        const uint32_t sB = sA + P.b_off;
+        // A: 128 rows x 8 units, this thread owns unit u of rows rg + 16 i
+        int slot, byte0;
+        if (P.cpo > 0) {
+          slot = j / P.cpo;
+          byte0 = (j % P.cpo) * 128 + u * 16;
+        } else {
+          slot = j * P.opc + u / P.upo;
+          byte0 = (u % P.upo) * 16;
+        }
+        const bool slot_ok = slot < na && byte0 < A.a_row_bytes;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int r = rg + 16 * i;
+          const int idx = slot_ok ? tab[slot * kTileM + r] : -1;
+          const uint8_t *src =
+              A.a_base + (idx >= 0 ? static_cast<int64_t>(idx) * A.a_row_stride + byte0 : 0);
+          cp_async_16(sA + sw128(r, u), src, idx >= 0 ? 16u : 0u);
+        }
+        // B: BN rows x 8 units
+        const int nb = A.BN >> 4;
+        for (int p = 0; p < nb; ++p) {
+          const int q = pt + 128 * p;
+          const int n = q >> 3;
+          const int uu = q & 7;
+          int kb, bbyte;
+          if (P.cpo > 0) {
+            kb = meta->k_list[slot];
+            bbyte = (j % P.cpo) * 128 + uu * 16;
+          } else {
+            const int sl = j * P.opc + uu / P.upo;
+            kb = sl < na ? meta->k_list[sl] : -1;
+            bbyte = (uu % P.upo) * 16;
+          }
+          const int ng = n0 + n;
+          const bool v = kb >= 0 && ng < A.n_total && bbyte < A.a_row_bytes;
+          const uint8_t *src =
+              A.b_base + (v ? static_cast<int64_t>(ng) * A.b_row_stride +
+                                  static_cast<int64_t>(kb) * A.b_off_stride + bbyte
+                            : 0);
+          cp_async_16(sB + sw128(n, uu), src, v ? 16u : 0u);
+        }
+        cp_async_commit();
+        ++chunk_ctr;
+        ++outstanding;
+        if (outstanding > kLag) {
+          cp_async_wait<kLag>();
+          fence_proxy_async_smem();
+          mbar_arrive(&full_bar[(chunk_ctr - outstanding) % S]);
+          --outstanding;
+        }
+      }
+      if (!ok) break;
+      mbar_arrive(&idx_empty[b]);
+    }
+    drain();
+  } else if (warp == 12) {
+    // ---------------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      int it = 0;
+      int64_t chunk_ctr = 0;
+      bool issued = false;
+      for (int64_t tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
+        const int b = it % kIdxStages;
+        const uint32_t ph = (it / kIdxStages) & 1;
+        if (!mbar_wait(&idx_full[b], ph, abort_flag)) {
+          flag_error(A.err, kErrWaitTimeout);
+          break;
+        }
+        const Meta *meta =
+            reinterpret_cast<const Meta *>(smem + P.idx_off + b * P.idx_buf_bytes + A.kv * kTileM * 4);
+        const int nch = meta->nchunks;
+        mbar_arrive(&idx_empty[b]);
+        const int ab = it & 1;
+        const uint32_t aph = (it >> 1) & 1;
+        if (!mbar_wait(&acc_empty[ab], aph ^ 1, abort_flag)) {
+          flag_error(A.err, kErrWaitTimeout);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + static_cast<uint32_t>(ab * A.BN);
+        if (nch == 0) {
+          mbar_arrive(&acc_full[ab]);
+          continue;
+        }
+        bool ok = true;
+        for (int j = 0; j < nch; ++j) {
+          const int s = static_cast<int>(chunk_ctr % S);
+          const uint32_t fph = static_cast<uint32_t>((chunk_ctr / S) & 1);
+          if (!mbar_wait(&full_bar[s], fph, abort_flag)) {
+            flag_error(A.err, kErrWaitTimeout);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sA = smem_base + s * P.stage_bytes;
+          const uint32_t sB = sA + P.b_off;
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            const uint64_t ad = make_sdesc(sA + kk * 32, 16, 1024);
+            const uint64_t bd = make_sdesc(sB + kk * 32, 16, 1024);
+            if constexpr (kF8)
+              mma_f8(d, ad, bd, P.idesc, (j | kk) != 0 ? 1u : 0u);
+            else
+              mma_f16(d, ad, bd, P.idesc, (j | kk) != 0 ? 1u : 0u);
+          }
+          issued = true;
+          mma_commit(&empty_bar[s]);
+          ++chunk_ctr;
+        }
+        if (!ok) break;
+        mma_commit(&acc_full[ab]);
+      }
+      if (issued) {
+        // make sure no tcgen05.mma is in flight before TMEM is released
+        mma_commit(drain_bar);
+        int never = 0;
+        if (!mbar_wait(drain_bar, 0, reinterpret_cast<volatile int *>(&never)))
+          flag_error(A.err, kErrWaitTimeout);
+      }
+    }
+  } else {
+    // ---------------------------------------------------------------- epilogue (warps 0-3)
+    const int r = threadIdx.x;  // TMEM lane == tile row
+    int it = 0;
+    const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
+    for (int64_t tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
+      const int64_t tile_m = tile / A.n_tiles;
+      const int n0 = static_cast<int>(tile % A.n_tiles) * A.BN;
+      const int64_t row_g = tile_m * kTileM + r;
+      const bool valid = row_g < A.M;
+      int sig = valid ? (A.argsort ? __ldg(A.argsort + row_g) : static_cast<int>(row_g)) : -1;
+      if (sig >= A.out_rows) sig = -1;
+      uint32_t km = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int64_t rr = tile_m * kTileM + q * 32 + lane;
+        if (rr < A.M) km |= A.mask ? __ldg(A.mask + rr) : 1u;
+      }
+#pragma unroll
+      for (int s = 16; s > 0; s >>= 1) km |= __shfl_xor_sync(0xffffffffu, km, s);
+      km &= A.mask_filter;
+      const int ab = it & 1;
+      const uint32_t aph = (it >> 1) & 1;
+      if (!mbar_wait(&acc_full[ab], aph, abort_flag)) {
+        flag_error(A.err, kErrWaitTimeout);
+        break;
+      }
+      tc_fence_after();
+      const bool write = valid && sig >= 0 && (A.is_fwd || km != 0);
+      const uint32_t tbase = tmem_base + lane_base + static_cast<uint32_t>(ab * A.BN);
+      for (int cc = 0; cc < A.BN; cc += 32) {
+        float acc[32];
+        if (A.BN - cc >= 32) {
+          if (km != 0) {
+            tmem_ld32(tbase + cc, acc);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) acc[i] = 0.f;
+          }
+          if (write) epilogue_cols<32, TOut>(P, acc, sig, n0 + cc);
+        } else {
+          if (km != 0) {
+            tmem_ld16(tbase + cc, acc);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[i] = 0.f;
+          }
+          if (write) epilogue_cols<16, TOut>(P, acc, sig, n0 + cc);
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&acc_empty[ab]);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 12) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem_base, P.tmem_cols);
+  }
+}
+
+template <bool kF8, typename TOut>
+cudaError_t launch_typed(const KParams &P, int grid, size_t smem, cudaStream_t stream) {
+  int lag = P.stages - 2;
+  if (lag > 4) lag = 4;
+  if (lag < 1) lag = 1;
+  void (*kern)(KParams) = nullptr;
+  switch (lag) {
+    case 1: kern = conv_rowgather_kernel<kF8, TOut, 1>; break;
+    case 2: kern = conv_rowgather_kernel<kF8, TOut, 2>; break;
+    case 3: kern = conv_rowgather_kernel<kF8, TOut, 3>; break;
+    default: kern = conv_rowgather_kernel<kF8, TOut, 4>; break;
+  }
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  kern<<<grid, kThreads, smem, stream>>>(P);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaStream_t stream) {
+  KParams P;
+  P.a = a;
+  const int64_t m_tiles = (a.M + kTileM - 1) / kTileM;
+  P.num_tiles = m_tiles * a.n_tiles;
+  if (a.a_row_bytes >= 128 || a.kv == 1) {
+    P.cpo = (a.a_row_bytes + 127) / 128;
+    P.opc = 1;
+    P.upo = 8;
+  } else {
+    P.cpo = 0;
+    P.opc = 128 / a.a_row_bytes;
+    P.upo = a.a_row_bytes / 16;
+  }
+  const uint32_t a_bytes = kTileM * 128;
+  const uint32_t b_bytes = static_cast<uint32_t>(a.BN) * 128;
+  P.stage_bytes = a_bytes + b_bytes;
+  P.b_off = a_bytes;
+  P.idx_buf_bytes = ((static_cast<uint32_t>(a.kv) * kTileM * 4 + sizeof(Meta)) + 127u) & ~127u;
+  const uint32_t idx_total = P.idx_buf_bytes * kIdxStages;
+  const uint32_t bar_bytes = 512;
+  const uint32_t budget = 227u * 1024u - 1024u - idx_total - bar_bytes;
+  int stages = static_cast<int>(budget / P.stage_bytes);
+  if (stages > 8) stages = 8;
+  if (stages < 2) return cudaErrorInvalidConfiguration;
+  P.stages = stages;
+  P.idx_off = P.stage_bytes * stages;
+  P.bar_off = P.idx_off + idx_total;
+  const size_t smem = 1024 + P.bar_off + bar_bytes;
+  uint32_t cols = 32;
+  while (cols < static_cast<uint32_t>(2 * a.BN)) cols <<= 1;
+  P.tmem_cols = cols;
+  if (P.num_tiles == 0) return cudaSuccess;
+  const int grid = static_cast<int>(P.num_tiles < num_sms ? P.num_tiles : num_sms);
+  if (a.in_dtype == 14) {
+    P.idesc = make_idesc(128, a.BN, 0u, false, false);
+    switch (a.out_dtype) {
+      case 0: return launch_typed<true, float>(P, grid, smem, stream);
+      case 7: return launch_typed<true, __half>(P, grid, smem, stream);
+      default: return launch_typed<true, __nv_bfloat16>(P, grid, smem, stream);
+    }
+  }
+  P.idesc = make_idesc(128, a.BN, a.in_dtype == 12 ? 1u : 0u, false, false);
+  switch (a.out_dtype) {
+    case 0: return launch_typed<false, float>(P, grid, smem, stream);
+    case 7: return launch_typed<false, __half>(P, grid, smem, stream);
+    case 12: return launch_typed<false, __nv_bfloat16>(P, grid, smem, stream);
+    default: break;
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace scb

@@ -1,0 +1,588 @@
+// conv_wgrad.cu - mask-implicit-GEMM sparse convolution, backward-weight, on
+// sm_100a tensor cores.
+//
+// Semantics follow the reference's wgrad path (cumm/gemm/blockmma/mma.py:580-765,
+// cumm/conv/sparse_iters.py:284-316, cumm/conv/kernel.py:890-897):
+//   dW[:, k, :] = sum over sorted rows r whose reduced mask word
+//                 mask[r / mask_width] has bit k (and k in mask_filter) of
+//                 dOut[sigma(r)]^T x In[indices[k][sigma(r)]]
+// with sigma = mask_argsort and In rows of index -1 contributing zero.
+// Offsets outside mask_filter are left untouched (kernel.py:893-896).
+//
+// B200 design: the reduction runs over gathered rows, so both operands are
+// staged MN-major: a 64-row chunk of gathered input rows (two 128-byte atoms =
+// 128 MN-elements: one or more filters' channels) is the M side and the
+// matching 64 dOut rows are the N side.  Every CTA owns a group of M-tiles
+// (up to 512 TMEM columns of fp32 accumulators) and a contiguous range of row
+// chunks; TMEM accumulates over the whole range, and the epilogue adds the
+// CTA's partial dW into an fp32 workspace with red.global.add (split over rows
+// without a serial semaphore, so there is no inter-CTA spin).  A finalize
+// kernel applies alpha/beta and converts to the weight dtype.
+// Warp roles are the same as the forward kernel: 0-3 epilogue, 4-7 cp.async
+// producers, 8-11 index loaders, 12 TMEM allocator + tcgen05.mma issuer.
+#include "kernels.h"
+
+namespace scb {
+namespace {
+
+constexpr int kThreads = 416;
+constexpr int kIdxStages = 3;
+constexpr int kRows = 64;  // reduction rows per stage
+
+struct WMeta {
+  int n_active;
+  uint32_t active_bits;  // bit j -> M-tile t0 + j active for this chunk
+  uint32_t grp[4];
+};
+
+struct WParams {
+  ConvWgradArgs a;
+  int n_chunks;        // ceil(N / 64)
+  int chunks_per_cta;
+  int n_groups;
+  int tiles_per_group;
+  int n_mtiles;
+  int n_atoms;
+  int cpa;             // 64-element c-blocks per filter (C >= 64), else 0
+  int fpa;             // filters per atom (C < 64)
+  int upf;             // 16-byte units per filter segment (C < 64)
+  int n_mma;           // MMA N (K rounded up to 64)
+  int stages;
+  uint32_t stage_bytes;
+  uint32_t b_off;
+  uint32_t idx_off;
+  uint32_t idx_buf_bytes;
+  uint32_t bar_off;
+  uint32_t tmem_cols;
+  uint32_t idesc;
+};
+
+__device__ __forceinline__ void flag_error(int *err, int bits) { atomicOr(err, bits); }
+
+// Filter and channel of element e (0..63) of atom a.
+__device__ __forceinline__ void atom_elem(const WParams &P, int a, int e, int &k, int &c) {
+  if (P.cpa > 0) {
+    k = a / P.cpa;
+    c = (a % P.cpa) * 64 + e;
+  } else {
+    const int C = P.a.C;
+    k = a * P.fpa + e / C;
+    c = e % C;
+  }
+}
+
+__device__ __forceinline__ void group_filters(const WParams &P, int g, int &k_lo, int &k_hi,
+                                              int &t0, int &t1) {
+  t0 = g * P.tiles_per_group;
+  t1 = min(t0 + P.tiles_per_group, P.n_mtiles);
+  const int a0 = 2 * t0;
+  const int a1 = min(2 * t1, P.n_atoms);  // exclusive
+  if (P.cpa > 0) {
+    k_lo = a0 / P.cpa;
+    k_hi = (a1 - 1) / P.cpa + 1;
+  } else {
+    k_lo = a0 * P.fpa;
+    k_hi = min(a1 * P.fpa, P.a.kv);
+  }
+}
+
+// Filter range covered by M-tile t.
+__device__ __forceinline__ uint32_t tile_filter_bits(const WParams &P, int t) {
+  const int a0 = 2 * t;
+  const int a1 = min(2 * t + 2, P.n_atoms);
+  int lo, hi;
+  if (P.cpa > 0) {
+    lo = a0 / P.cpa;
+    hi = (a1 - 1) / P.cpa + 1;
+  } else {
+    lo = a0 * P.fpa;
+    hi = min(a1 * P.fpa, P.a.kv);
+  }
+  const uint32_t upto_hi = hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u);
+  return upto_hi & ~((1u << lo) - 1u);
+}
+
+template <int kLag>
+__global__ void __maxnreg__(152) conv_wgrad_kernel(const __grid_constant__ WParams P) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw_u32 = smem_u32(smem_raw);
+  const uint32_t pad = (1024u - (raw_u32 & 1023u)) & 1023u;
+  uint8_t *smem = smem_raw + pad;
+  const uint32_t smem_base = raw_u32 + pad;
+  const ConvWgradArgs &A = P.a;
+
+  const int S = P.stages;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + P.bar_off);
+  uint64_t *full_bar = bars;
+  uint64_t *empty_bar = bars + S;
+  uint64_t *idx_full = bars + 2 * S;
+  uint64_t *idx_empty = idx_full + kIdxStages;
+  uint64_t *acc_full = idx_empty + kIdxStages;
+  uint64_t *drain_bar = acc_full + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain_bar + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  uint32_t *used_tiles = reinterpret_cast<uint32_t *>(tmem_slot + 2);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int g = blockIdx.y;
+  int k_lo, k_hi, t0, t1;
+  group_filters(P, g, k_lo, k_hi, t0, t1);
+  const int c_begin = blockIdx.x * P.chunks_per_cta;
+  const int c_end = min(c_begin + P.chunks_per_cta, P.n_chunks);
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < S; ++i) {
+      mbar_init(&full_bar[i], 128);
+      mbar_init(&empty_bar[i], 1);
+    }
+    for (int i = 0; i < kIdxStages; ++i) {
+      mbar_init(&idx_full[i], 128);
+      mbar_init(&idx_empty[i], 129);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(drain_bar, 1);
+    *abort_flag = 0;
+    *used_tiles = 0;
+    fence_mbar_init();
+  }
+  if (warp == 12) {
+    tmem_alloc(tmem_slot, P.tmem_cols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp >= 8 && warp < 12) {
+    // ---------------------------------------------------------------- index loaders
+    const int t = threadIdx.x - 256;
+    const int r = t & 63;       // row of the chunk
+    const int half = t >> 6;    // filter parity handled by this thread
+    int it = 0;
+    for (int c = c_begin; c < c_end; ++c, ++it) {
+      const int b = it % kIdxStages;
+      const uint32_t ph = (it / kIdxStages) & 1;
+      if (!mbar_wait(&idx_empty[b], ph ^ 1, abort_flag)) {
+        flag_error(A.err, kErrWaitTimeout);
+        break;
+      }
+      uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
+      int *tab = reinterpret_cast<int *>(buf);          // [F][64]
+      int *sig_tab = tab + 32 * kRows;                   // [64]
+      WMeta *meta = reinterpret_cast<WMeta *>(sig_tab + kRows);
+      const int64_t row = static_cast<int64_t>(c) * kRows + r;
+      const bool valid = row < A.N;
+      int sig = valid ? (A.argsort ? __ldg(A.argsort + row) : static_cast<int>(row)) : -1;
+      if (valid && (sig < 0 || sig >= A.dout_rows)) {
+        flag_error(A.err, kErrBadIndex);
+        sig = -1;
+      }
+      uint32_t word = 0;
+      if (valid) {
+        if (A.mask) {
+          const int64_t wi = row / A.mask_width;
+          if (wi < A.mask_count) word = __ldg(A.mask + wi);
+        } else {
+          word = 0xffffffffu;
+        }
+      }
+      word &= A.mask_filter;
+      // this warp covers rows (r & 32) .. +31; the partner half of the chunk is
+      // the same rows one warp over, so OR the words of both 32-row halves
+      // without a cross-warp barrier (rows r and r ^ 32 share a mask word
+      // unless mask_width < 64; read both explicitly)
+      uint32_t w_other = 0;
+      {
+        const int64_t row2 = static_cast<int64_t>(c) * kRows + (r ^ 32);
+        if (row2 < A.N) {
+          if (A.mask) {
+            const int64_t wi = row2 / A.mask_width;
+            if (wi < A.mask_count) w_other = __ldg(A.mask + wi);
+          } else {
+            w_other = 0xffffffffu;
+          }
+        }
+        w_other &= A.mask_filter;
+      }
+      uint32_t gw = word | w_other;
+#pragma unroll
+      for (int s = 16; s > 0; s >>= 1) gw |= __shfl_xor_sync(0xffffffffu, gw, s);
+      if (half == 0) sig_tab[r] = sig;
+      const uint32_t cm = gw;
+      int vals[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int k = k_lo + 2 * q + half;
+        int v = -1;
+        if (k < k_hi && ((word >> k) & 1u) && sig >= 0) {
+          if (A.indices)
+            v = __ldg(A.indices + static_cast<int64_t>(k) * A.N + sig);
+          else
+            v = A.b_inds ? __ldg(A.b_inds + row) : static_cast<int>(row);
+        }
+        vals[q] = v;
+      }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int k = k_lo + 2 * q + half;
+        if (k < k_hi) {
+          int v = vals[q];
+          if (v < -1 || v >= A.in_rows) {
+            flag_error(A.err, kErrBadIndex);
+            v = -1;
+          }
+          tab[(k - k_lo) * kRows + r] = v;
+        }
+      }
+      if (t == 0) {
+        uint32_t bits = 0;
+        for (int tt = t0; tt < t1; ++tt)
+          if (tile_filter_bits(P, tt) & cm) bits |= 1u << (tt - t0);
+        meta->active_bits = bits;
+        meta->n_active = __popc(bits);
+      }
+      // grp[] of this buffer is rewritten only after idx_empty, i.e. after all
+      // loader threads passed the named barrier of this chunk
+      mbar_arrive(&idx_full[b]);
+    }
+  } else if (warp >= 4 && warp < 8) {
+    // ---------------------------------------------------------------- producers
+    const int pt = threadIdx.x - 128;
+    const int u = pt & 7;
+    const int rg = pt >> 3;  // 0..15
+    int it = 0;
+    int64_t stage_ctr = 0;
+    int outstanding = 0;
+    bool ok = true;
+    auto drain = [&]() {
+      cp_async_wait_all();
+      fence_proxy_async_smem();
+      while (outstanding > 0) {
+        mbar_arrive(&full_bar[(stage_ctr - outstanding) % S]);
+        --outstanding;
+      }
+    };
+    const int n_b_atoms = P.n_mma / 64;
+    for (int c = c_begin; c < c_end && ok; ++c, ++it) {
+      const int b = it % kIdxStages;
+      const uint32_t ph = (it / kIdxStages) & 1;
+      if (!mbar_try_wait(&idx_full[b], ph)) {
+        drain();
+        if (!mbar_wait(&idx_full[b], ph, abort_flag)) {
+          flag_error(A.err, kErrWaitTimeout);
+          break;
+        }
+      }
+      const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
+      const int *tab = reinterpret_cast<const int *>(buf);
+      const int *sig_tab = tab + 32 * kRows;
+      const WMeta *meta = reinterpret_cast<const WMeta *>(sig_tab + kRows);
+      uint32_t bits = meta->active_bits;
+      while (bits) {
+        const int j = __ffs(bits) - 1;
+        bits &= bits - 1;
+        const int tt = t0 + j;
+        const int s = static_cast<int>(stage_ctr % S);
+        const uint32_t eph = static_cast<uint32_t>((stage_ctr / S) & 1);
+        if (!mbar_wait(&empty_bar[s], eph ^ 1, abort_flag)) {
+          flag_error(A.err, kErrWaitTimeout);
+          ok = false;
+          break;
+        }
+        const uint32_t sA = smem_base + s * P.stage_bytes;
+        const uint32_t sB = sA + P.b_off;
+        // M side: two atoms x 64 rows; unit u of rows rg + 16 i
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int a = 2 * tt + h;
+          int k, byte0;
+          if (P.cpa > 0) {
+            k = a / P.cpa;
+            byte0 = (a % P.cpa) * 128 + u * 16;
+          } else {
+            k = a * P.fpa + u / P.upf;
+            byte0 = (u % P.upf) * 16;
+          }
+          const bool atom_ok = a < P.n_atoms && k < A.kv;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int r = rg + 16 * i;
+            const int idx = atom_ok ? tab[(k - k_lo) * kRows + r] : -1;
+            const uint8_t *src =
+                A.input + (idx >= 0 ? static_cast<int64_t>(idx) * A.in_ld * 2 + byte0 : 0);
+            cp_async_16(sA + h * 8192 + sw128(r, u), src, idx >= 0 ? 16u : 0u);
+          }
+        }
+        // N side: n_b_atoms atoms x 64 rows of dOut[sigma(r)]
+        for (int na = 0; na < n_b_atoms; ++na) {
+          const bool col_ok = na * 64 + u * 8 < A.K;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int r = rg + 16 * i;
+            const int sg = sig_tab[r];
+            const bool v = col_ok && sg >= 0;
+            const uint8_t *src =
+                A.dout + (v ? static_cast<int64_t>(sg) * A.dout_ld * 2 + na * 128 + u * 16 : 0);
+            cp_async_16(sB + na * 8192 + sw128(r, u), src, v ? 16u : 0u);
+          }
+        }
+        cp_async_commit();
+        ++stage_ctr;
+        ++outstanding;
+        if (outstanding > kLag) {
+          cp_async_wait<kLag>();
+          fence_proxy_async_smem();
+          mbar_arrive(&full_bar[(stage_ctr - outstanding) % S]);
+          --outstanding;
+        }
+      }
+      if (!ok) break;
+      mbar_arrive(&idx_empty[b]);
+    }
+    drain();
+  } else if (warp == 12) {
+    // ---------------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      int it = 0;
+      int64_t stage_ctr = 0;
+      uint32_t started = 0;
+      bool ok = true;
+      for (int c = c_begin; c < c_end && ok; ++c, ++it) {
+        const int b = it % kIdxStages;
+        const uint32_t ph = (it / kIdxStages) & 1;
+        if (!mbar_wait(&idx_full[b], ph, abort_flag)) {
+          flag_error(A.err, kErrWaitTimeout);
+          break;
+        }
+        const WMeta *meta = reinterpret_cast<const WMeta *>(smem + P.idx_off + b * P.idx_buf_bytes +
+                                                            (32 * kRows + kRows) * 4);
+        uint32_t bits = meta->active_bits;
+        mbar_arrive(&idx_empty[b]);
+        while (bits) {
+          const int j = __ffs(bits) - 1;
+          bits &= bits - 1;
+          const int s = static_cast<int>(stage_ctr % S);
+          const uint32_t fph = static_cast<uint32_t>((stage_ctr / S) & 1);
+          if (!mbar_wait(&full_bar[s], fph, abort_flag)) {
+            flag_error(A.err, kErrWaitTimeout);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sA = smem_base + s * P.stage_bytes;
+          const uint32_t sB = sA + P.b_off;
+          const uint32_t d = tmem_base + static_cast<uint32_t>(j * P.n_mma);
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            const uint64_t ad = make_sdesc(sA + kk * 2048, 8192, 1024);
+            const uint64_t bd = make_sdesc(sB + kk * 2048, 8192, 1024);
+            const uint32_t acc = ((started >> j) & 1u) || kk > 0 ? 1u : 0u;
+            mma_f16(d, ad, bd, P.idesc, acc);
+          }
+          started |= 1u << j;
+          mma_commit(&empty_bar[s]);
+          ++stage_ctr;
+        }
+      }
+      if (started) {
+        // all MMAs complete before the epilogue reads TMEM
+        mma_commit(drain_bar);
+        int never = 0;
+        if (!mbar_wait(drain_bar, 0, reinterpret_cast<volatile int *>(&never))) {
+          flag_error(A.err, kErrWaitTimeout);
+          started = 0;
+        }
+        tc_fence_after();
+      }
+      *used_tiles = started;
+      tc_fence_before();
+      mbar_arrive(acc_full);  // release: used_tiles and the finished accumulators
+    }
+  } else {
+    // ---------------------------------------------------------------- epilogue (warps 0-3)
+    if (mbar_wait(acc_full, 0, abort_flag)) {
+      tc_fence_after();
+      const uint32_t used = *reinterpret_cast<volatile uint32_t *>(used_tiles);
+      const int m = threadIdx.x;  // TMEM lane = M element
+      const int h = m >> 6;
+      const int e = m & 63;
+      const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
+      for (int j = 0; j < t1 - t0; ++j) {
+        if (!((used >> j) & 1u)) continue;
+        const int a = 2 * (t0 + j) + h;
+        int k = 0, ch = 0;
+        if (a < P.n_atoms) atom_elem(P, a, e, k, ch);
+        const bool ok = a < P.n_atoms && k < A.kv && ((A.mask_filter >> k) & 1u);
+        for (int n0 = 0; n0 < P.n_mma; n0 += 32) {
+          float v[32];
+          tmem_ld32(tmem_base + lane_base + static_cast<uint32_t>(j * P.n_mma + n0), v);
+          if (ok) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+              const int n = n0 + i;
+              if (n < A.K) atomicAdd(A.ws + (static_cast<int64_t>(n) * A.kv + k) * A.C + ch, v[i]);
+            }
+          }
+        }
+      }
+    } else {
+      flag_error(A.err, kErrWaitTimeout);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 12) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem_base, P.tmem_cols);
+  }
+}
+
+template <typename TOut>
+__global__ void wgrad_finalize_kernel(const float *ws, TOut *out, int64_t out_ld, int64_t total,
+                                      int kv, int C, uint32_t mask_filter, EpiParams e) {
+  const int64_t row_len = static_cast<int64_t>(kv) * C;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t row = i / row_len;
+    const int64_t col = i % row_len;
+    const int k = static_cast<int>(col / C);
+    if (!((mask_filter >> k) & 1u)) continue;
+    float v = e.alpha * ws[i];
+    if (e.beta != 0.f && e.src != nullptr)
+      v = fmaf(e.beta, to_f32(static_cast<const TOut *>(e.src)[row * e.src_ld + col]), v);
+    out[row * out_ld + col] = from_f32<TOut>(apply_act(v, e.act_type, e.act_alpha));
+  }
+}
+
+template <typename T>
+__global__ void transpose_weight_kernel(const T *w, T *wt, int K, int kv, int C) {
+  // w[K, kv, C] -> wt[C, kv, K]
+  const int64_t total = static_cast<int64_t>(K) * kv * C;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(i % C);
+    const int k = static_cast<int>((i / C) % kv);
+    const int ko = static_cast<int>(i / (static_cast<int64_t>(C) * kv));
+    wt[(static_cast<int64_t>(c) * kv + k) * K + ko] = w[i];
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t stream) {
+  WParams P;
+  P.a = a;
+  P.n_chunks = static_cast<int>((a.N + kRows - 1) / kRows);
+  if (P.n_chunks == 0) return cudaSuccess;
+  if (a.C >= 64) {
+    P.cpa = a.C / 64;
+    P.fpa = 1;
+    P.upf = 8;
+    P.n_atoms = a.kv * P.cpa;
+  } else {
+    P.cpa = 0;
+    P.fpa = 64 / a.C;
+    P.upf = a.C / 8;
+    P.n_atoms = (a.kv + P.fpa - 1) / P.fpa;
+  }
+  P.n_mtiles = (P.n_atoms + 1) / 2;
+  P.n_mma = ((a.K + 63) / 64) * 64;
+  int per_group = 512 / P.n_mma;
+  if (per_group > 16) per_group = 16;
+  if (per_group > P.n_mtiles) per_group = P.n_mtiles;
+  P.tiles_per_group = per_group;
+  P.n_groups = (P.n_mtiles + per_group - 1) / per_group;
+  int splits = (num_sms + P.n_groups - 1) / P.n_groups;
+  if (splits > P.n_chunks) splits = P.n_chunks;
+  P.chunks_per_cta = (P.n_chunks + splits - 1) / splits;
+  splits = (P.n_chunks + P.chunks_per_cta - 1) / P.chunks_per_cta;
+  const uint32_t a_bytes = 2 * 8192;
+  const uint32_t b_bytes = static_cast<uint32_t>(P.n_mma / 64) * 8192;
+  P.stage_bytes = a_bytes + b_bytes;
+  P.b_off = a_bytes;
+  P.idx_buf_bytes = ((32 * kRows + kRows) * 4 + sizeof(WMeta) + 127) & ~127u;
+  const uint32_t idx_total = P.idx_buf_bytes * kIdxStages;
+  const uint32_t bar_bytes = 512;
+  const uint32_t budget = 227u * 1024u - 1024u - idx_total - bar_bytes;
+  int stages = static_cast<int>(budget / P.stage_bytes);
+  if (stages > 8) stages = 8;
+  if (stages < 2) return cudaErrorInvalidConfiguration;
+  P.stages = stages;
+  P.idx_off = P.stage_bytes * stages;
+  P.bar_off = P.idx_off + idx_total;
+  const size_t smem = 1024 + P.bar_off + bar_bytes;
+  uint32_t cols = 32;
+  while (cols < static_cast<uint32_t>(per_group * P.n_mma)) cols <<= 1;
+  P.tmem_cols = cols;
+  P.idesc = make_idesc(128, P.n_mma, 1u, true, true);  // bf16 only (checked by the caller)
+  int lag = stages - 2;
+  if (lag > 4) lag = 4;
+  if (lag < 1) lag = 1;
+  void (*kern)(WParams) = nullptr;
+  switch (lag) {
+    case 1: kern = conv_wgrad_kernel<1>; break;
+    case 2: kern = conv_wgrad_kernel<2>; break;
+    case 3: kern = conv_wgrad_kernel<3>; break;
+    default: kern = conv_wgrad_kernel<4>; break;
+  }
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  dim3 grid(splits, P.n_groups);
+  kern<<<grid, kThreads, smem, stream>>>(P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wgrad_finalize(const float *ws, void *out, int64_t out_ld, int out_dtype,
+                                  int K, int kv, int C, uint32_t mask_filter, const EpiParams &e,
+                                  cudaStream_t stream) {
+  const int64_t total = static_cast<int64_t>(K) * kv * C;
+  const int threads = 256;
+  int blocks = static_cast<int>((total + threads - 1) / threads);
+  if (blocks > 4096) blocks = 4096;
+  if (blocks < 1) blocks = 1;
+  switch (out_dtype) {
+    case 0:
+      wgrad_finalize_kernel<float><<<blocks, threads, 0, stream>>>(
+          ws, static_cast<float *>(out), out_ld, total, kv, C, mask_filter, e);
+      break;
+    case 7:
+      wgrad_finalize_kernel<__half><<<blocks, threads, 0, stream>>>(
+          ws, static_cast<__half *>(out), out_ld, total, kv, C, mask_filter, e);
+      break;
+    case 12:
+      wgrad_finalize_kernel<__nv_bfloat16><<<blocks, threads, 0, stream>>>(
+          ws, static_cast<__nv_bfloat16 *>(out), out_ld, total, kv, C, mask_filter, e);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_weight(const void *w, void *wt, int K, int kv, int C, int esize,
+                                    cudaStream_t stream) {
+  const int64_t total = static_cast<int64_t>(K) * kv * C;
+  const int threads = 256;
+  int blocks = static_cast<int>((total + threads - 1) / threads);
+  if (blocks > 4096) blocks = 4096;
+  if (blocks < 1) blocks = 1;
+  if (esize == 2)
+    transpose_weight_kernel<uint16_t><<<blocks, threads, 0, stream>>>(
+        static_cast<const uint16_t *>(w), static_cast<uint16_t *>(wt), K, kv, C);
+  else if (esize == 1)
+    transpose_weight_kernel<uint8_t><<<blocks, threads, 0, stream>>>(
+        static_cast<const uint8_t *>(w), static_cast<uint8_t *>(wt), K, kv, C);
+  else if (esize == 4)
+    transpose_weight_kernel<float><<<blocks, threads, 0, stream>>>(
+        static_cast<const float *>(w), static_cast<float *>(wt), K, kv, C);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+}  // namespace scb

@@ -1,0 +1,161 @@
+// kernels.h - host-side launch interfaces between the C ABI (api.cu) and the
+// kernel translation units.  No torch types; plain pointers and sizes.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace scb {
+
+// ------------------------------------------------------------------ conv fwd / dgrad (tcgen05)
+// Row-gather implicit GEMM: for every 128-row tile of the sorted row order,
+//   out[sigma(r), n] = epi( sum_{k in tile mask} sum_c A[idx[k][sigma(r)], c] * B[n, k, c] )
+// A = input (fwd) or dOut (dgrad) rows; B = weight [K, kv, C] (fwd) or its
+// transpose [C, kv, K] (dgrad).
+struct ConvRowGatherArgs {
+  const uint8_t *a_base;
+  int64_t a_rows;
+  int a_row_bytes;           // bytes of one A row (reduction elements per offset * esize)
+  int64_t a_row_stride;      // bytes between A rows
+  const uint8_t *b_base;
+  int64_t b_row_stride;      // bytes between B rows (kv * reduction * esize)
+  int b_off_stride;          // bytes between offsets inside a B row
+  int n_total;               // GEMM N
+  int BN;                    // N tile (multiple of 16, <= 256)
+  int n_tiles;
+  int64_t M;                 // rows (indices.dim(1))
+  int kv;
+  const uint32_t *mask;
+  const int32_t *argsort;
+  const int32_t *indices;
+  uint32_t *mask_out;
+  int tile_m_desp;           // 32, 64 or 128
+  uint32_t mask_filter;
+  int reverse;
+  int is_fwd;
+  void *out;
+  int64_t out_ld;
+  int in_dtype;              // 12 bf16, 7 f16, 14 e4m3 (kind::f8f6f4)
+  int out_dtype;             // SC_* dtype of out/src/bias
+  EpiParams epi;
+  int *err;
+  // dense / ShuffleAC GEMM mode (indices == nullptr, kv == 1, mask == nullptr):
+  // A row of sorted row r = a_inds ? a_inds[r] : r, output row = argsort ? argsort[r] : r
+  const int32_t *a_inds;
+  int64_t out_rows;          // bound for output rows
+};
+cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaStream_t stream);
+
+// dgrad weight transposition W[K, kv, C] -> Wt[C, kv, K] (16-bit or 8-bit elements)
+cudaError_t launch_transpose_weight(const void *w, void *wt, int K, int kv, int C, int esize,
+                                    cudaStream_t stream);
+
+// ------------------------------------------------------------------ conv wgrad (tcgen05)
+// dW[K, kv, C] (fp32 workspace accumulation) = sum over rows of
+//   dOut[sigma(r)]^T x In[idx[k][sigma(r)]], rows gated by mask[r / mask_width].
+struct ConvWgradArgs {
+  const uint8_t *dout;       // [rows_out, K]
+  int64_t dout_rows;
+  int64_t dout_ld;           // elements
+  const uint8_t *input;      // [rows_in, C]
+  int64_t in_rows;
+  int64_t in_ld;             // elements
+  int K;
+  int C;
+  int kv;
+  int64_t N;                 // rows (indices.dim(1))
+  const uint32_t *mask;      // reduced masks (fwd mask_output)
+  int64_t mask_count;
+  int mask_width;
+  uint32_t mask_filter;
+  const int32_t *argsort;
+  const int32_t *indices;
+  float *ws;                 // [K, kv, C] fp32, zeroed
+  int *err;
+  // ShuffleAB GEMM mode (indices == nullptr, kv == 1): input row of sorted row r
+  // is b_inds ? b_inds[r] : r; dOut row is argsort ? argsort[r] : r; mask may be null
+  const int32_t *b_inds;
+};
+cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t stream);
+
+// out[K, kv, C] = act(alpha * ws + beta * src) for offsets in mask_filter
+// (others untouched); src rows have stride src_ld (0 = [C] bias row), out rows
+// have stride out_ld (elements, per K row).
+cudaError_t launch_wgrad_finalize(const float *ws, void *out, int64_t out_ld, int out_dtype,
+                                  int K, int kv, int C, uint32_t mask_filter, const EpiParams &e,
+                                  cudaStream_t stream);
+
+// ------------------------------------------------------------------ SIMT fp32 conv
+struct ConvSimtArgs {
+  int op;                    // 0 fwd, 1 dgrad, 2 wgrad
+  const float *a;            // gathered operand (fwd: input, dgrad: dout, wgrad: dout)
+  int64_t a_rows;
+  const float *b;            // fwd/dgrad: weight [K, kv, C]; wgrad: input [rows, C]
+  int64_t b_rows;
+  float *out;                // fwd: [.., K]; dgrad: [.., C]; wgrad: ws [K, kv, C]
+  int C, K, kv;
+  int64_t M;
+  const uint32_t *mask;
+  int64_t mask_count;
+  const int32_t *argsort;
+  const int32_t *indices;
+  uint32_t *mask_out;
+  int tile_m_desp;
+  int mask_width;
+  uint32_t mask_filter;
+  int reverse;
+  EpiParams epi;
+  int *err;
+};
+cudaError_t launch_conv_simt(const ConvSimtArgs &a, cudaStream_t stream);
+
+// ------------------------------------------------------------------ GEMM
+struct GemmArgs {
+  int shuffle;               // 0 none, 1 AC, 2 AB
+  int trans_a, trans_b;
+  int64_t m, n, k;
+  const uint8_t *a;
+  int64_t lda;
+  const uint8_t *b;
+  int64_t ldb;
+  void *c;
+  int64_t ldc;
+  const int32_t *a_inds, *b_inds, *c_inds;
+  int64_t a_rows, b_rows;
+  int in_dtype;              // SC_BFLOAT16 / SC_FLOAT16 / SC_FLOAT32
+  int out_dtype;
+  EpiParams epi;
+  float *ws;                 // fp32 [m, n] accumulation workspace (ShuffleAB / trans_a)
+  int *err;
+};
+cudaError_t launch_gemm(const GemmArgs &a, int num_sms, cudaStream_t stream);
+int64_t gemm_workspace_bytes(const GemmArgs &a);
+
+// ------------------------------------------------------------------ pair builder
+struct PairBuildArgs {
+  const int32_t *coords;
+  int64_t n_in;
+  int batch;
+  int spatial[3];
+  int ksize[3];
+  int stride[3];
+  int padding[3];
+  int dilation[3];
+  int out_spatial[3];
+  int subm;
+  int *err;
+};
+int64_t pairs_workspace_bytes(int64_t n_in, int kv, int subm);
+cudaError_t build_subm_pairs(const PairBuildArgs &a, int32_t *pairs_fwd, int32_t *pairs_bwd,
+                             uint32_t *mask_fwd, void *ws, int64_t ws_bytes, cudaStream_t s);
+cudaError_t build_conv_outputs(const PairBuildArgs &a, int64_t *n_out, void *ws,
+                               int64_t ws_bytes, cudaStream_t s);
+cudaError_t build_conv_pairs(const PairBuildArgs &a, int64_t n_out, int32_t *out_coords,
+                             int32_t *pairs_fwd, int32_t *pairs_bwd, uint32_t *mask_fwd,
+                             uint32_t *mask_bwd, void *ws, int64_t ws_bytes, cudaStream_t s);
+int64_t sort_workspace_bytes(int64_t n);
+cudaError_t sort_masks_split(uint32_t *data, int64_t n, uint32_t split_mask, int32_t *argsort,
+                             void *ws, int64_t ws_bytes, cudaStream_t s);
+
+}  // namespace scb

@@ -1,0 +1,250 @@
+"""GPU parity of the sparse conv kernels (through the C ABI via
+ConvMainUnitTest.implicit_gemm2) against the FP64 oracle."""
+import numpy as np
+import pytest
+import torch
+
+from cumm import tensorview as tv
+from cumm import voxelgen as vg
+from cumm.tensorview.gemm import ConvOpType
+from oracle import conv_oracle as co
+from oracle import pairs_oracle as po
+from tests.helpers import TORCH, conv, dev, find_desp, to64, u32
+
+pytestmark = pytest.mark.gpu
+
+TOL_16 = 2e-3   # bf16/f16 operands, fp32 accumulation: norm-relative vs FP64
+TOL_32 = 1e-5   # fp32 SIMT path
+
+
+def _cloud(n, grid=24, seed=0):
+    return vg.uniform_voxels(n, grid, seed)
+
+
+def _subm(n, grid, seed):
+    coords = _cloud(n, grid, seed)
+    pf, pb, m = po.subm_pairs(coords, (grid, grid, grid))
+    return coords, pf, pb, m
+
+
+def _assert_close(y, ref, tol):
+    nr, mr, ma = co.rel_err(y, ref)
+    assert nr <= tol, (nr, mr, ma)
+
+
+@pytest.mark.parametrize("dt", [tv.bfloat16, tv.float16])
+@pytest.mark.parametrize("n,grid,C,K", [(3000, 24, 64, 64), (1000, 16, 32, 48), (777, 16, 16, 16),
+                                        (2000, 20, 128, 128), (500, 12, 96, 32)])
+@pytest.mark.parametrize("tile_m", [128, 32])
+def test_fwd_tcgen05(dt, n, grid, C, K, tile_m):
+    coords, pf, pb, m = _subm(n, grid, n)
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((n, C)).astype(np.float32)
+    w = vg.kaiming_uniform(K, 27, C, 2)
+    xt, wt = dev(x, TORCH[dt]), dev(w, TORCH[dt])
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    out = torch.zeros((n, K), dtype=TORCH[dt], device="cuda")
+    mo = tv.zeros([(n + tile_m - 1) // tile_m], tv.uint32, 0)
+    conv(ConvOpType.kForward, find_desp(ConvOpType.kForward, "Tcgen05", dt, dt, dt, tile_m),
+         xt, wt, out, pf, ms, order, mask_output=mo)
+    ref, mo_ref = co.conv_fwd_masked(to64(xt), to64(wt), pf, ms, order, tile_m)
+    _assert_close(to64(out), ref, TOL_16)
+    assert np.array_equal(mo.numpy(), mo_ref)
+
+
+@pytest.mark.parametrize("dt", [tv.bfloat16, tv.float16])
+@pytest.mark.parametrize("n,grid,C,K", [(3000, 24, 64, 64), (1000, 16, 48, 32), (600, 12, 16, 16)])
+def test_dgrad_tcgen05(dt, n, grid, C, K):
+    coords, pf, pb, m = _subm(n, grid, n + 1)
+    rng = np.random.default_rng(3)
+    dy = rng.standard_normal((n, K)).astype(np.float32)
+    w = vg.kaiming_uniform(K, 27, C, 4)
+    dyt, wt = dev(dy, TORCH[dt]), dev(w, TORCH[dt])
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    din = torch.zeros((n, C), dtype=TORCH[dt], device="cuda")
+    conv(ConvOpType.kBackwardInput,
+         find_desp(ConvOpType.kBackwardInput, "Tcgen05", dt, dt, dt, 128),
+         din, wt, dyt, pb, ms, order, reverse_mask=True)
+    ref = co.conv_dgrad_masked(to64(dyt), to64(wt), pb, ms, order, 128, reverse_mask=True)
+    _assert_close(to64(din), ref, TOL_16)
+
+
+@pytest.mark.parametrize("dw_dt", [tv.bfloat16, tv.float32])
+@pytest.mark.parametrize("n,grid,C,K", [(3000, 24, 64, 64), (1500, 16, 32, 32), (800, 12, 128, 64),
+                                        (700, 12, 16, 16)])
+def test_wgrad_tcgen05(dw_dt, n, grid, C, K):
+    coords, pf, pb, m = _subm(n, grid, n + 2)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((n, C)).astype(np.float32)
+    dy = rng.standard_normal((n, K)).astype(np.float32)
+    xt, dyt = dev(x, torch.bfloat16), dev(dy, torch.bfloat16)
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    mo = co.tile_masks(ms, 128).astype(np.uint32)
+    dw = torch.zeros((K, 27, C), dtype=TORCH[dw_dt], device="cuda")
+    desp = find_desp(ConvOpType.kBackwardWeight, "Tcgen05", tv.bfloat16, dw_dt, tv.bfloat16, 128)
+    conv(ConvOpType.kBackwardWeight, desp, xt, dw, dyt, pf, mo, order, mask_width=128)
+    ref = co.conv_wgrad_masked(to64(dyt), to64(xt), pf, mo, 128, order, 27)
+    _assert_close(to64(dw), ref, TOL_16 if dw_dt == tv.bfloat16 else 2e-5)
+
+
+def test_split_two_launches_equals_single():
+    """MaskSplitImplicitGemm: split filters with beta=1 on the second launch
+    (main_real_spconv.py:273-294) equals one launch with all offsets."""
+    n, grid, C, K = 4000, 24, 64, 64
+    coords, pf, pb, m = _subm(n, grid, 9)
+    rng = np.random.default_rng(9)
+    xt = dev(rng.standard_normal((n, C)).astype(np.float32), torch.bfloat16)
+    wt = dev(vg.kaiming_uniform(K, 27, C, 9), torch.bfloat16)
+    desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.float32, 128)
+    out1 = torch.zeros((n, K), dtype=torch.float32, device="cuda")
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    conv(ConvOpType.kForward, desp, xt, wt, out1, pf, ms, order)
+    out2 = torch.zeros((n, K), dtype=torch.float32, device="cuda")
+    for j, sm in enumerate(po.split_masks(27, 2)):
+        msj, oj = po.sort_by_key_split(m, sm)
+        conv(ConvOpType.kForward, desp, xt, wt, out2, pf, msj, oj, mask_filter=sm,
+             beta=1.0 if j else 0.0)
+    _assert_close(to64(out2), to64(out1), 1e-6)
+    ref = co.fwd_gather_gemm_scatter(to64(xt), to64(wt), pf)
+    _assert_close(to64(out1), ref, 1e-5)
+
+
+def test_fwd_epilogue_bias_act():
+    n, grid, C, K = 1500, 16, 32, 64
+    coords, pf, pb, m = _subm(n, grid, 10)
+    rng = np.random.default_rng(10)
+    xt = dev(rng.standard_normal((n, C)).astype(np.float32), torch.bfloat16)
+    wt = dev(vg.kaiming_uniform(K, 27, C, 10), torch.bfloat16)
+    bias = dev(rng.standard_normal(K).astype(np.float32), torch.bfloat16)
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 128)
+    for act_type, act_alpha in ((1, 0.0), (3, 0.1), (2, 0.0)):
+        out = torch.zeros((n, K), dtype=torch.bfloat16, device="cuda")
+        conv(ConvOpType.kForward, desp, xt, wt, out, pf, ms, order, alpha=0.5, beta=1.0,
+             bias=bias, act_type=act_type, act_alpha=act_alpha)
+        ref, _ = co.conv_fwd_masked(to64(xt), to64(wt), pf, ms, order, 128, alpha=0.5, beta=1.0,
+                                    bias=to64(bias), act_type=act_type, act_alpha=act_alpha)
+        _assert_close(to64(out), ref, TOL_16)
+
+
+def test_fwd_fp8_scale_epilogue():
+    n, grid, C, K = 2000, 20, 64, 128
+    coords, pf, pb, m = _subm(n, grid, 11)
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((n, C)).astype(np.float32)
+    w = vg.kaiming_uniform(K, 27, C, 11)
+    sx = np.abs(x).max() / 448.0
+    sw = np.abs(w).reshape(K, -1).max(1) / 448.0
+    xq = dev(x / sx, torch.float8_e4m3fn)
+    wq = dev(w / sw[:, None, None], torch.float8_e4m3fn)
+    scale = dev((sx * sw).astype(np.float32))
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    out = torch.zeros((n, K), dtype=torch.bfloat16, device="cuda")
+    desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.float_e4m3, tv.float_e4m3, tv.bfloat16, 128)
+    conv(ConvOpType.kForward, desp, xq, wq, out, pf, ms, order, scale=scale)
+    ref, _ = co.conv_fwd_masked(to64(xq), to64(wq), pf, ms, order, 128,
+                                scale=(sx * sw).astype(np.float64))
+    _assert_close(to64(out), ref, TOL_16)
+
+
+@pytest.mark.parametrize("op", [ConvOpType.kForward, ConvOpType.kBackwardInput,
+                                ConvOpType.kBackwardWeight])
+def test_simt_fp32(op):
+    """The fp32 path meets 1e-5 norm-relative (20k voxels in 64^3, C=K=32 is
+    the workload; a smaller cloud keeps the test short)."""
+    n, grid, C, K = 5000, 40, 32, 32
+    coords, pf, pb, m = _subm(n, grid, 12)
+    rng = np.random.default_rng(12)
+    x = rng.standard_normal((n, C)).astype(np.float32)
+    w = vg.kaiming_uniform(K, 27, C, 12)
+    dy = rng.standard_normal((n, K)).astype(np.float32)
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    desp = find_desp(op, "Simt", tv.float32, tv.float32, tv.float32, 32 if op != 2 else 32)
+    if op == ConvOpType.kForward:
+        out = torch.zeros((n, K), device="cuda")
+        conv(op, desp, dev(x), dev(w), out, pf, ms, order)
+        ref, _ = co.conv_fwd_masked(x, w, pf, ms, order, 32)
+        _assert_close(to64(out), ref, TOL_32)
+    elif op == ConvOpType.kBackwardInput:
+        din = torch.zeros((n, C), device="cuda")
+        conv(op, desp, din, dev(w), dev(dy), pb, ms, order, reverse_mask=True)
+        ref = co.conv_dgrad_masked(dy, w, pb, ms, order, 32, reverse_mask=True)
+        _assert_close(to64(din), ref, TOL_32)
+    else:
+        mo = co.tile_masks(ms, 32).astype(np.uint32)
+        dw = torch.zeros((K, 27, C), device="cuda")
+        conv(op, desp, dev(x), dw, dev(dy), pf, mo, order, mask_width=32)
+        ref = co.conv_wgrad_masked(dy, x, pf, mo, 32, order, 27)
+        _assert_close(to64(dw), ref, TOL_32)
+
+
+def test_edge_cases():
+    desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 128)
+    # all-empty masks: outputs get the epilogue of a zero accumulator (beta * bias)
+    n, C, K = 300, 64, 64
+    pf = np.full((27, n), -1, np.int32)
+    m = np.zeros(n, np.uint32)
+    order = np.arange(n, dtype=np.int32)
+    x = dev(np.ones((n, C), np.float32), torch.bfloat16)
+    w = dev(np.ones((K, 27, C), np.float32), torch.bfloat16)
+    out = torch.full((n, K), 7.0, dtype=torch.bfloat16, device="cuda")
+    conv(ConvOpType.kForward, desp, x, w, out, pf, m, order)
+    assert torch.all(out == 0)
+    # dgrad with empty masks writes nothing
+    din = torch.full((n, C), 3.0, dtype=torch.bfloat16, device="cuda")
+    dd = find_desp(ConvOpType.kBackwardInput, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 128)
+    conv(ConvOpType.kBackwardInput, dd, din, w, out, pf, m, order, reverse_mask=True)
+    assert torch.all(din == 3.0)
+    # N = 0
+    e = torch.zeros((0, C), dtype=torch.bfloat16, device="cuda")
+    eo = torch.zeros((0, K), dtype=torch.bfloat16, device="cuda")
+    conv(ConvOpType.kForward, desp, e, w, eo, np.zeros((27, 0), np.int32), np.zeros(0, np.uint32),
+         np.zeros(0, np.int32))
+
+
+def test_bad_index_reported():
+    """A gather index beyond the input raises a device error instead of reading
+    out of bounds (the kernel checks every index and zero-fills)."""
+    n, C, K = 256, 64, 64
+    desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 128)
+    pf = np.full((27, n), -1, np.int32)
+    pf[13] = np.arange(n)
+    pf[13, 5] = n + 100  # out of range
+    m = np.full(n, 1 << 13, np.uint32)
+    x = dev(np.ones((n, C), np.float32), torch.bfloat16)
+    w = dev(np.ones((K, 27, C), np.float32), torch.bfloat16)
+    out = torch.zeros((n, K), dtype=torch.bfloat16, device="cuda")
+    with pytest.raises(RuntimeError, match="device error"):
+        conv(ConvOpType.kForward, desp, x, w, out, pf, m, np.arange(n, dtype=np.int32))
+
+
+@pytest.mark.parametrize("seed", [0])
+def test_lidar_200k_fwd_dgrad_wgrad(seed):
+    """The 200k-voxel LiDAR-like C=K=64 bf16 layer: fwd, dgrad, wgrad against
+    the FP64 oracle at 2e-3."""
+    n, C, K = 200000, 64, 64
+    coords = vg.lidar_voxels(n, seed=seed)
+    pf, pb, m = po.subm_pairs(coords, vg.KITTI_SHAPE)
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    rng = np.random.default_rng(seed)
+    xt = dev(rng.standard_normal((n, C)).astype(np.float32), torch.bfloat16)
+    wt = dev(vg.kaiming_uniform(K, 27, C, seed), torch.bfloat16)
+    dyt = dev(rng.standard_normal((n, K)).astype(np.float32), torch.bfloat16)
+    out = torch.zeros((n, K), dtype=torch.bfloat16, device="cuda")
+    mo = tv.zeros([(n + 127) // 128], tv.uint32, 0)
+    conv(ConvOpType.kForward,
+         find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 128),
+         xt, wt, out, pf, ms, order, mask_output=mo)
+    x64, w64, dy64 = to64(xt), to64(wt), to64(dyt)
+    ref = co.fwd_gather_gemm_scatter(x64, w64, pf)
+    _assert_close(to64(out), ref, TOL_16)
+    din = torch.zeros((n, C), dtype=torch.bfloat16, device="cuda")
+    conv(ConvOpType.kBackwardInput,
+         find_desp(ConvOpType.kBackwardInput, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 128),
+         din, wt, dyt, pb, ms, order, reverse_mask=True)
+    _assert_close(to64(din), co.dgrad_gather_gemm_scatter(dy64, w64, pb), TOL_16)
+    dw = torch.zeros((K, 27, C), dtype=torch.float32, device="cuda")
+    conv(ConvOpType.kBackwardWeight,
+         find_desp(ConvOpType.kBackwardWeight, "Tcgen05", tv.bfloat16, tv.float32, tv.bfloat16, 128),
+         xt, dw, dyt, pf, mo.numpy(), order, mask_width=128)
+    _assert_close(to64(dw), co.wgrad_gather_gemm_scatter(dy64, x64, pf), TOL_16)

@@ -1,0 +1,137 @@
+"""CPU tests of the host side: the C ABI library loads and exports every
+symbol include/cumm_b200.h declares, argument validation maps to the
+reference's exception types, and the Python mirror of the reference
+interface (tv.Tensor, descriptors, mnk helpers) behaves like cumm's."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from cumm import _lib
+from cumm import tensorview as tv
+from cumm.conv.main import ConvMainUnitTest, get_all_conv_algo_desp, implicit_gemm_mnk
+from cumm.gemm.main import GemmMainUnitTest, extract_mnk, get_all_algo_desp
+from cumm.tensorview.gemm import ConvAlgoDesp, ConvOpType, ConvParams, GemmAlgoDesp
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def _declared():
+    text = (ROOT / "include" / "cumm_b200.h").read_text()
+    return sorted(set(re.findall(r"^(?:int|const char \*)\s*(sc_\w+)\(", text, re.M)))
+
+
+def test_library_exports_header_symbols():
+    lib = _lib.load()
+    names = _declared()
+    assert len(names) >= 13
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_lib.EXPORTS)
+    assert lib.sc_version().decode().startswith("cumm_b200")
+
+
+def _fake_conv(op=0, **kw):
+    cp = _lib.ConvParamsC()
+    cp.op_type, cp.algo = op, _lib.SC_ALGO_TCGEN05
+    cp.dtype_input = cp.dtype_weight = cp.dtype_output = tv.bfloat16
+    cp.tile_m, cp.tile_k, cp.kv = 128, 64, 27
+    cp.n_in = cp.n_out = cp.N = 1000
+    cp.C = cp.K = 64
+    for f in ("input", "weight", "output", "indices", "mask", "mask_argsort"):
+        setattr(cp, f, 0x1000)
+    cp.mask_count = 1000
+    cp.mask_width = 128
+    for k, v in kw.items():
+        setattr(cp, k, v)
+    return cp
+
+
+def _ws(cp):
+    lib = _lib.load()
+    n = ctypes.c_int64(-1)
+    rc = lib.sc_conv_workspace_size(ctypes.byref(cp), ctypes.byref(n))
+    return rc, n.value, lib.sc_last_error().decode()
+
+
+def test_conv_validation_codes():
+    assert _ws(_fake_conv())[:2] == (0, 0)
+    rc, n, _ = _ws(_fake_conv(1))
+    assert rc == 0 and n == 64 * 27 * 64 * 2          # dgrad: transposed weight
+    rc, n, _ = _ws(_fake_conv(2))
+    assert rc == 0 and n == 64 * 27 * 64 * 4          # wgrad: fp32 accumulation
+    rc, _, msg = _ws(_fake_conv(0, N=999))
+    assert rc == _lib.SC_RUNTIME and "output.dim(0)" in msg
+    rc, _, msg = _ws(_fake_conv(2, mask_width=100))
+    assert rc == _lib.SC_RUNTIME and "mask_width" in msg
+    rc, _, msg = _ws(_fake_conv(0, C=20))
+    assert rc == _lib.SC_RUNTIME and "Can't Found Algorithm" in msg
+    rc, _, msg = _ws(_fake_conv(0, indices=None))
+    assert rc == _lib.SC_RUNTIME
+    rc, _, msg = _ws(_fake_conv(0, tile_m=256))
+    assert rc == _lib.SC_RUNTIME
+    rc, _, msg = _ws(_fake_conv(0, output_add=0x2000))
+    assert rc == _lib.SC_INVALID_ARG
+    with pytest.raises(ValueError):
+        _lib.check(_lib.SC_INVALID_ARG)
+    with pytest.raises(RuntimeError):
+        _lib.check(_lib.SC_RUNTIME)
+
+
+def test_null_params():
+    lib = _lib.load()
+    assert lib.sc_conv_implicit_gemm(None) == _lib.SC_INVALID_ARG
+    assert lib.sc_gemm_matmul(None) == _lib.SC_INVALID_ARG
+
+
+def test_tensor_mirror():
+    a = np.arange(12, dtype=np.uint32).reshape(3, 4) | np.uint32(1 << 31)
+    t = tv.from_numpy(a)
+    assert t.dtype == tv.uint32 and t.shape == [3, 4] and t.dim(1) == 4 and t.device == -1
+    assert np.array_equal(t.numpy(), a)
+    assert t.slice_first_axis(1, 2).shape == [1, 4]
+    z = tv.zeros([5], tv.bfloat16)
+    assert z.itemsize == 2 and z.numpy().sum() == 0
+    f = tv.full([2, 2], 0xffffffff, tv.uint32)
+    assert np.all(f.numpy() == 0xffffffff)
+    assert tv.Tensor().empty()
+
+
+def test_descriptors_and_mnk():
+    d = ConvAlgoDesp(3, ConvOpType.kBackwardWeight)
+    assert d.conv_iwo_012_to_abc(ConvOpType.kBackwardInput) == [2, 1, 0]
+    assert d.gemm_abc_012_to_iwo(ConvOpType.kBackwardWeight) == [2, 0, 1]
+    assert implicit_gemm_mnk(ConvOpType.kForward, 100, 32, 64, 27) == (100, 64, 32 * 27)
+    assert implicit_gemm_mnk(ConvOpType.kBackwardInput, 100, 32, 64, 27) == (100, 32, 64 * 27)
+    assert implicit_gemm_mnk(ConvOpType.kBackwardWeight, 100, 32, 64, 27) == (64, 32 * 27, 100)
+    assert ConvMainUnitTest.extract_mnk(0, 100, 32, 64, 27) == [100, 64, 864]
+    desps = get_all_conv_algo_desp()
+    assert len(desps) > 10
+    for dd in desps:
+        name = repr(dd)
+        assert dd.mask_sparse and ("_SK" in name)
+    fwd = [x for x in desps if x.op_type == ConvOpType.kForward and x.algo == "Tcgen05"][0]
+    assert fwd.supported(1000, 64, 64 * 27, 64, 64, 128)
+    wg = [x for x in desps if x.op_type == ConvOpType.kBackwardWeight and x.algo == "Tcgen05"][0]
+    assert not wg.supported(64, 64 * 27, 1000, 64, 64, 100)
+    assert wg.query_conv_workspace_size(64, 64 * 27, 1000, 1, 27) == 64 * 27 * 64 * 4
+    assert extract_mnk([100, 32], [32, 48], False, False, False) == (100, 48, 32)
+    assert extract_mnk([32, 100], [48, 32], True, True, False) == (100, 48, 32)
+    assert extract_mnk([1000, 64], [1000, 32], True, False, False, 2, [500]) == (64, 32, 500)
+    assert GemmMainUnitTest.align_to_power2(100) == 128
+    gd = get_all_algo_desp()
+    assert any(x.shuffle_type == 1 for x in gd) and any(x.shuffle_type == 2 for x in gd)
+    g = GemmAlgoDesp()
+    with pytest.raises(RuntimeError):
+        g.check_valid()
+
+
+def test_ops_need_cuda_no_cpu_fallback():
+    if torch.cuda.is_available():
+        pytest.skip("has a GPU")
+    p = ConvParams(3, ConvOpType.kForward)
+    with pytest.raises(RuntimeError, match="CUDA device"):
+        ConvMainUnitTest().implicit_gemm2(p)
