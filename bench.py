@@ -314,9 +314,9 @@ def run_b200(args, rank, world, dist):
         dw_h.copy_(dwd, non_blocking=True)
         torch.cuda.synchronize()
 
-    for _ in range(2):
+    n_e2e = 0 if args.no_e2e else max(3, min(args.steps, 20))
+    for _ in range(2 if n_e2e else 0):
         e2e_step()
-    n_e2e = max(3, min(args.steps, 20))
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -327,7 +327,7 @@ def run_b200(args, rank, world, dist):
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / n_e2e
+    e2e_ms = e0.elapsed_time(e1) / max(n_e2e, 1)
     if dist is not None:
         t = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -390,6 +390,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end loop (profiling)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -187,7 +187,7 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
     return SC_OK;
   }
   // backward weight
-  if (di != SC_BFLOAT16 || dout != SC_BFLOAT16 || !(dw == SC_BFLOAT16 || dw == SC_FLOAT32 || dw == SC_FLOAT16))
+  if (!is16(di) || dout != di || !(dw == SC_BFLOAT16 || dw == SC_FLOAT32 || dw == SC_FLOAT16))
     return fail(SC_RUNTIME, "Can't Found Algorithm for params: %s %s %s", dtype_name(di),
                 dtype_name(dw), dtype_name(dout));
   if (!(p->C % 64 == 0 || p->C == 8 || p->C == 16 || p->C == 32) || p->K % 8 || p->K > 256)
@@ -407,6 +407,7 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     a.ws = static_cast<float *>(p->workspace);
     a.err = err;
     a.b_inds = nullptr;
+    a.in_dtype = p->dtype_input;
     e = scb::launch_conv_wgrad(a, sms, s);
     if (e != cudaSuccess) return cuda_fail(e, "conv wgrad launch");
     scb::EpiParams ep{};

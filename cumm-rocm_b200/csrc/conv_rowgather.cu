@@ -17,23 +17,31 @@
 // sub-tile (32/64/128) gates its own rows, which keeps results identical to a
 // tile_shape[0]-row kernel even for masks inconsistent with the index table.
 //
-// B200 design (one persistent CTA per SM, 13 warps, warp-specialised):
+// B200 design (one persistent CTA per SM, 17 warps, warp-specialised):
 //   warps 0-3   epilogue: TMEM -> registers -> permuted row stores
-//   warps 4-7   producers: 16-byte cp.async gathers of A rows and B slabs into
-//               SWIZZLE_128B shared-memory stages (one 128-byte reduction chunk
-//               per stage), completion handed to the MMA warp by mbarrier
-//   warps 8-11  index loaders: mask / argsort / indices of the next tiles into
+//   warps 4-11  producers: 16-byte cp.async gathers of the A rows that have a
+//               pair into SWIZZLE_128B shared-memory stages (one 128-byte
+//               reduction chunk per stage); rows without a pair are
+//               zero-filled copies (no memory request; a shared store would
+//               need a proxy fence that waits on the thread's copies in
+//               flight); the weight slab arrives by one 2-D TMA load.
+//               Measured on B200: scattered 128-byte rows reach ~100 GB/s per
+//               SM through cp.async from 8+ warps, TMA tile::gather4 only
+//               ~13 GB/s per issuing warp, so the gather stays on cp.async.
+//   warps 12-15 index loaders: mask / argsort / indices of the next tiles into
 //               a 3-deep shared-memory ring (hides the argsort->index latency)
-//   warp 12     TMEM allocator + single-thread tcgen05.mma issuer into a
+//   warp 16     TMEM allocator + single-thread tcgen05.mma issuer into a
 //               double-buffered fp32 TMEM accumulator (128 lanes x BN columns)
 // Every mbarrier wait is bounded (globaltimer) and raises a CTA abort flag
 // plus kErrWaitTimeout instead of spinning forever.
+#include <cuda.h>
+
 #include "kernels.h"
 
 namespace scb {
 namespace {
 
-constexpr int kThreads = 416;
+constexpr int kThreads = 544;
 constexpr int kIdxStages = 3;
 constexpr int kTileM = 128;
 
@@ -47,6 +55,8 @@ struct Meta {
 };
 
 struct KParams {
+  CUtensorMap tmap_a;  // gathered rows [a_rows, red] (TMA path)
+  CUtensorMap tmap_b;  // B rows [n_total, kv * red] (TMA path)
   ConvRowGatherArgs a;
   int64_t num_tiles;
   int cpo;            // chunks per offset (a_row_bytes >= 128), else 0
@@ -107,14 +117,14 @@ __device__ __forceinline__ void store_row(TOut *p, const float *v) {
 template <int n, typename TOut>
 __device__ __forceinline__ void epilogue_cols(const KParams &P, float *acc, int64_t orow, int col) {
   const EpiParams &e = P.a.epi;
-  float src[32];
+  float src[n];
   const bool use_src = e.beta != 0.f && e.src != nullptr;
   if (use_src) {
     const TOut *s = reinterpret_cast<const TOut *>(e.src) + orow * e.src_ld + col;
     load_src<n, TOut>(s, src);
   }
   if (e.mode == 1) {
-    float bias[32];
+    float bias[n];
     if (e.bias != nullptr) load_src<n, TOut>(reinterpret_cast<const TOut *>(e.bias) + col, bias);
 #pragma unroll
     for (int i = 0; i < n; ++i) {
@@ -150,8 +160,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
 }
 
 // ------------------------------------------------------------------ kernel
-template <bool kF8, typename TOut, int kLag>
-__global__ void __maxnreg__(152)
+// Warp roles (17 warps):
+constexpr int kEpiWarps = 4;     // warps 0-3
+constexpr int kProdWarp0 = 4;    // warps 4-11
+constexpr int kProdWarps = 8;
+constexpr int kLoadWarp0 = 12;   // warps 12-15
+constexpr int kMmaWarp = 16;
+constexpr int kProdThreads = kProdWarps * 32;
+
+template <bool kF8, typename TOut, bool kTma>
+__global__ void __maxnreg__(96)
     conv_rowgather_kernel(const __grid_constant__ KParams P) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_u32 = smem_u32(smem_raw);
@@ -177,12 +195,14 @@ __global__ void __maxnreg__(152)
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < S; ++i) {
-      mbar_init(&full_bar[i], 128);
+      // every producer thread arrives through cp.async.mbarrier.arrive.noinc;
+      // with the TMA weight load one more arrive.expect_tx
+      mbar_init(&full_bar[i], kProdThreads + (kTma ? 1 : 0));
       mbar_init(&empty_bar[i], 1);
     }
     for (int i = 0; i < kIdxStages; ++i) {
       mbar_init(&idx_full[i], 128);
-      mbar_init(&idx_empty[i], 129);
+      mbar_init(&idx_empty[i], kProdWarps + 1);
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(&acc_full[i], 1);
@@ -192,7 +212,7 @@ __global__ void __maxnreg__(152)
     *abort_flag = 0;
     fence_mbar_init();
   }
-  if (warp == 12) {
+  if (warp == kMmaWarp) {
     tmem_alloc(tmem_slot, P.tmem_cols);
     tmem_relinquish();
   }
@@ -201,9 +221,9 @@ __global__ void __maxnreg__(152)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  if (warp >= 8 && warp < 12) {
+  if (warp >= kLoadWarp0 && warp < kLoadWarp0 + 4) {
     // ---------------------------------------------------------------- index loaders
-    const int r = threadIdx.x - 256;  // row inside the tile
+    const int r = threadIdx.x - kLoadWarp0 * 32;  // row inside the tile
     const int lw = r >> 5;
     int it = 0;
     for (int64_t tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
@@ -263,28 +283,34 @@ __global__ void __maxnreg__(152)
         tm = __brev(tm) >> (32 - A.kv);
         sub = __brev(sub) >> (32 - A.kv);
       }
-      int vals[32];
+      // 16 offsets per batch keeps the loads in flight without a 32-entry array
 #pragma unroll
-      for (int k = 0; k < 32; ++k) {
-        int v = -1;
-        if (k < A.kv && ((tm >> k) & 1u) && sig >= 0 && ((sub >> k) & 1u)) {
-          if (A.indices)
-            v = __ldg(A.indices + static_cast<int64_t>(k) * A.M + sig);
-          else
-            v = A.a_inds ? __ldg(A.a_inds + row_g) : static_cast<int>(row_g);
-        }
-        vals[k] = v;
-      }
+      for (int kb = 0; kb < 32; kb += 16) {
+        int vals[16];
 #pragma unroll
-      for (int k = 0; k < 32; ++k) {
-        if (k < A.kv && ((tm >> k) & 1u)) {
-          int v = vals[k];
-          if (v < -1 || v >= A.a_rows) {
-            flag_error(A.err, kErrBadIndex);
-            v = -1;
+        for (int q = 0; q < 16; ++q) {
+          const int k = kb + q;
+          int v = -1;
+          if (k < A.kv && ((tm >> k) & 1u) && sig >= 0 && ((sub >> k) & 1u)) {
+            if (A.indices)
+              v = __ldg(A.indices + static_cast<int64_t>(k) * A.M + sig);
+            else
+              v = A.a_inds ? __ldg(A.a_inds + row_g) : static_cast<int>(row_g);
           }
-          const int slot = __popc(tm & ((1u << k) - 1u));
-          tab[slot * kTileM + r] = v;
+          vals[q] = v;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int k = kb + q;
+          if (k < A.kv && ((tm >> k) & 1u)) {
+            int v = vals[q];
+            if (v < -1 || v >= A.a_rows) {
+              flag_error(A.err, kErrBadIndex);
+              v = -1;
+            }
+            const int slot = __popc(tm & ((1u << k) - 1u));
+            tab[slot * kTileM + r] = v;
+          }
         }
       }
       if (r == 0) {
@@ -300,37 +326,32 @@ __global__ void __maxnreg__(152)
         meta->tilemask = tm;
         meta->nchunks = P.cpo > 0 ? na * P.cpo : (na + P.opc - 1) / P.opc;
       }
-      // the group words are re-read by nobody after this point; all writes of
-      // this thread are released by its arrive
       mbar_arrive(&idx_full[b]);
     }
-  } else if (warp >= 4 && warp < 8) {
+  } else if (warp >= kProdWarp0 && warp < kProdWarp0 + kProdWarps) {
     // ---------------------------------------------------------------- producers
-    const int pt = threadIdx.x - 128;
+    // 256 threads; thread pt owns 16-byte unit u of rows rg + 32 i (i < 4).
+    // Rows with a pair are fetched with 16-byte cp.async; rows without one are
+    // zero-filled cp.async (src-size 0, no memory request).  With TMA the
+    // weight slab is one 2-D tiled load issued by thread 0.
+    const int pt = threadIdx.x - kProdWarp0 * 32;
     const int u = pt & 7;
     const int rg = pt >> 3;
+    const int esz = kF8 ? 1 : 2;
+    const int box = 128 / esz;
+    const uint32_t b_tx = static_cast<uint32_t>(A.BN) * 128;
     int it = 0;
     int64_t chunk_ctr = 0;
-    int outstanding = 0;
     bool ok = true;
-    auto drain = [&]() {
-      cp_async_wait_all();
-      fence_proxy_async_smem();
-      while (outstanding > 0) {
-        const int64_t c = chunk_ctr - outstanding;
-        mbar_arrive(&full_bar[c % S]);
-        --outstanding;
-      }
-    };
     for (int64_t tile = blockIdx.x; tile < P.num_tiles && ok; tile += gridDim.x, ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
-      if (!mbar_try_wait(&idx_full[b], ph)) {
-        drain();
-        if (!mbar_wait(&idx_full[b], ph, abort_flag)) {
-          flag_error(A.err, kErrWaitTimeout);
-          break;
-        }
+      int w_ok = 1;
+      if (lane == 0) w_ok = mbar_wait(&idx_full[b], ph, abort_flag) ? 1 : 0;
+      w_ok = __shfl_sync(0xffffffffu, w_ok, 0);
+      if (!w_ok) {
+        if (lane == 0) flag_error(A.err, kErrWaitTimeout);
+        break;
       }
       const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
       const int *tab = reinterpret_cast<const int *>(buf);
@@ -341,14 +362,16 @@ __global__ void __maxnreg__(152)
       for (int j = 0; j < nch; ++j) {
         const int s = static_cast<int>(chunk_ctr % S);
         const uint32_t eph = static_cast<uint32_t>((chunk_ctr / S) & 1);
-        if (!mbar_wait(&empty_bar[s], eph ^ 1, abort_flag)) {
-          flag_error(A.err, kErrWaitTimeout);
+        int e_ok = 1;
+        if (lane == 0) e_ok = mbar_wait(&empty_bar[s], eph ^ 1, abort_flag) ? 1 : 0;
+        e_ok = __shfl_sync(0xffffffffu, e_ok, 0);
+        if (!e_ok) {
+          if (lane == 0) flag_error(A.err, kErrWaitTimeout);
           ok = false;
           break;
         }
         const uint32_t sA = smem_base + s * P.stage_bytes;
         const uint32_t sB = sA + P.b_off;
-        // A: 128 rows x 8 units, this thread owns unit u of rows rg + 16 i
         int slot, byte0;
         if (P.cpo > 0) {
           slot = j / P.cpo;
@@ -357,53 +380,62 @@ __global__ void __maxnreg__(152)
           slot = j * P.opc + u / P.upo;
           byte0 = (u % P.upo) * 16;
         }
+        if constexpr (kTma) {
+          if (pt == 0) {
+            mbar_arrive_expect_tx(&full_bar[s], b_tx);
+            const int cb = j % P.cpo;
+            const int xb = meta->k_list[slot] * (A.b_off_stride / esz) + cb * box;
+            tma_load_2d(sB, &P.tmap_b, xb, n0, &full_bar[s]);
+          }
+        }
         const bool slot_ok = slot < na && byte0 < A.a_row_bytes;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int r = rg + 16 * i;
+        for (int i = 0; i < 4; ++i) {
+          const int r = rg + 32 * i;
           const int idx = slot_ok ? tab[slot * kTileM + r] : -1;
-          const uint8_t *src =
-              A.a_base + (idx >= 0 ? static_cast<int64_t>(idx) * A.a_row_stride + byte0 : 0);
-          cp_async_16(sA + sw128(r, u), src, idx >= 0 ? 16u : 0u);
-        }
-        // B: BN rows x 8 units
-        const int nb = A.BN >> 4;
-        for (int p = 0; p < nb; ++p) {
-          const int q = pt + 128 * p;
-          const int n = q >> 3;
-          const int uu = q & 7;
-          int kb, bbyte;
-          if (P.cpo > 0) {
-            kb = meta->k_list[slot];
-            bbyte = (j % P.cpo) * 128 + uu * 16;
+          const uint32_t dst = sA + sw128(r, u);
+          if (idx >= 0) {
+            cp_async_16(dst, A.a_base + static_cast<int64_t>(idx) * A.a_row_stride + byte0, 16u);
           } else {
-            const int sl = j * P.opc + uu / P.upo;
-            kb = sl < na ? meta->k_list[sl] : -1;
-            bbyte = (uu % P.upo) * 16;
+            cp_async_16(dst, A.a_base, 0u);  // zero fill, no memory request
           }
-          const int ng = n0 + n;
-          const bool v = kb >= 0 && ng < A.n_total && bbyte < A.a_row_bytes;
-          const uint8_t *src =
-              A.b_base + (v ? static_cast<int64_t>(ng) * A.b_row_stride +
-                                  static_cast<int64_t>(kb) * A.b_off_stride + bbyte
-                            : 0);
-          cp_async_16(sB + sw128(n, uu), src, v ? 16u : 0u);
         }
-        cp_async_commit();
+        if constexpr (!kTma) {
+          // B: BN rows x 8 units over the 256 producer threads
+          for (int q = pt; q < A.BN * 8; q += kProdThreads) {
+            const int n = q >> 3;
+            const int uu = q & 7;
+            int kb, bbyte;
+            if (P.cpo > 0) {
+              kb = meta->k_list[slot];
+              bbyte = (j % P.cpo) * 128 + uu * 16;
+            } else {
+              const int sl = j * P.opc + uu / P.upo;
+              kb = sl < na ? meta->k_list[sl] : -1;
+              bbyte = (uu % P.upo) * 16;
+            }
+            const int ng = n0 + n;
+            const uint32_t dst = sB + sw128(n, uu);
+            if (kb >= 0 && ng < A.n_total && bbyte < A.a_row_bytes) {
+              cp_async_16(dst,
+                          A.b_base + static_cast<int64_t>(ng) * A.b_row_stride +
+                              static_cast<int64_t>(kb) * A.b_off_stride + bbyte,
+                          16u);
+            } else {
+              cp_async_16(dst, A.b_base, 0u);  // zero fill, no memory request
+            }
+          }
+        }
+        // the stage's full barrier counts this thread once its copies land
+        cp_async_mbar_arrive_noinc(&full_bar[s]);
         ++chunk_ctr;
-        ++outstanding;
-        if (outstanding > kLag) {
-          cp_async_wait<kLag>();
-          fence_proxy_async_smem();
-          mbar_arrive(&full_bar[(chunk_ctr - outstanding) % S]);
-          --outstanding;
-        }
       }
       if (!ok) break;
-      mbar_arrive(&idx_empty[b]);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&idx_empty[b]);
     }
-    drain();
-  } else if (warp == 12) {
+    cp_async_wait_all();
+  } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
       int it = 0;
@@ -468,7 +500,7 @@ __global__ void __maxnreg__(152)
           flag_error(A.err, kErrWaitTimeout);
       }
     }
-  } else {
+  } else if (warp < kEpiWarps) {
     // ---------------------------------------------------------------- epilogue (warps 0-3)
     const int r = threadIdx.x;  // TMEM lane == tile row
     int it = 0;
@@ -498,25 +530,15 @@ __global__ void __maxnreg__(152)
       tc_fence_after();
       const bool write = valid && sig >= 0 && (A.is_fwd || km != 0);
       const uint32_t tbase = tmem_base + lane_base + static_cast<uint32_t>(ab * A.BN);
-      for (int cc = 0; cc < A.BN; cc += 32) {
-        float acc[32];
-        if (A.BN - cc >= 32) {
-          if (km != 0) {
-            tmem_ld32(tbase + cc, acc);
-          } else {
-#pragma unroll
-            for (int i = 0; i < 32; ++i) acc[i] = 0.f;
-          }
-          if (write) epilogue_cols<32, TOut>(P, acc, sig, n0 + cc);
+      for (int cc = 0; cc < A.BN; cc += 16) {
+        float acc[16];
+        if (km != 0) {
+          tmem_ld16(tbase + cc, acc);
         } else {
-          if (km != 0) {
-            tmem_ld16(tbase + cc, acc);
-          } else {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) acc[i] = 0.f;
-          }
-          if (write) epilogue_cols<16, TOut>(P, acc, sig, n0 + cc);
+          for (int i = 0; i < 16; ++i) acc[i] = 0.f;
         }
+        if (write) epilogue_cols<16, TOut>(P, acc, sig, n0 + cc);
       }
       tc_fence_before();
       mbar_arrive(&acc_empty[ab]);
@@ -525,7 +547,7 @@ __global__ void __maxnreg__(152)
 
   tc_fence_before();
   __syncthreads();
-  if (warp == 12) {
+  if (warp == kMmaWarp) {
     __syncwarp();
     tc_fence_after();
     tmem_dealloc(tmem_base, P.tmem_cols);
@@ -533,17 +555,9 @@ __global__ void __maxnreg__(152)
 }
 
 template <bool kF8, typename TOut>
-cudaError_t launch_typed(const KParams &P, int grid, size_t smem, cudaStream_t stream) {
-  int lag = P.stages - 2;
-  if (lag > 4) lag = 4;
-  if (lag < 1) lag = 1;
-  void (*kern)(KParams) = nullptr;
-  switch (lag) {
-    case 1: kern = conv_rowgather_kernel<kF8, TOut, 1>; break;
-    case 2: kern = conv_rowgather_kernel<kF8, TOut, 2>; break;
-    case 3: kern = conv_rowgather_kernel<kF8, TOut, 3>; break;
-    default: kern = conv_rowgather_kernel<kF8, TOut, 4>; break;
-  }
+cudaError_t launch_typed(const KParams &P, bool tma, int grid, size_t smem, cudaStream_t stream) {
+  void (*kern)(KParams) =
+      tma ? conv_rowgather_kernel<kF8, TOut, true> : conv_rowgather_kernel<kF8, TOut, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
@@ -587,19 +601,28 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
   P.tmem_cols = cols;
   if (P.num_tiles == 0) return cudaSuccess;
   const int grid = static_cast<int>(P.num_tiles < num_sms ? P.num_tiles : num_sms);
+  // TMA weight slabs: whole 128-byte reduction chunks (no packing of small offsets)
+  bool tma = false;
+  if (P.cpo > 0) {
+    const int esz = a.in_dtype == 14 ? 1 : 2;
+    const uint32_t box = 128u / esz;
+    const uint64_t red = static_cast<uint64_t>(a.a_row_bytes) / esz;
+    tma = encode_tmap_2d(&P.tmap_b, a.in_dtype, a.b_base, red * a.kv, a.n_total,
+                         static_cast<uint64_t>(a.b_row_stride), box, a.BN);
+  }
   if (a.in_dtype == 14) {
     P.idesc = make_idesc(128, a.BN, 0u, false, false);
     switch (a.out_dtype) {
-      case 0: return launch_typed<true, float>(P, grid, smem, stream);
-      case 7: return launch_typed<true, __half>(P, grid, smem, stream);
-      default: return launch_typed<true, __nv_bfloat16>(P, grid, smem, stream);
+      case 0: return launch_typed<true, float>(P, tma, grid, smem, stream);
+      case 7: return launch_typed<true, __half>(P, tma, grid, smem, stream);
+      default: return launch_typed<true, __nv_bfloat16>(P, tma, grid, smem, stream);
     }
   }
   P.idesc = make_idesc(128, a.BN, a.in_dtype == 12 ? 1u : 0u, false, false);
   switch (a.out_dtype) {
-    case 0: return launch_typed<false, float>(P, grid, smem, stream);
-    case 7: return launch_typed<false, __half>(P, grid, smem, stream);
-    case 12: return launch_typed<false, __nv_bfloat16>(P, grid, smem, stream);
+    case 0: return launch_typed<false, float>(P, tma, grid, smem, stream);
+    case 7: return launch_typed<false, __half>(P, tma, grid, smem, stream);
+    case 12: return launch_typed<false, __nv_bfloat16>(P, tma, grid, smem, stream);
     default: break;
   }
   return cudaErrorInvalidValue;

@@ -18,14 +18,19 @@
 // CTA's partial dW into an fp32 workspace with red.global.add (split over rows
 // without a serial semaphore, so there is no inter-CTA spin).  A finalize
 // kernel applies alpha/beta and converts to the weight dtype.
-// Warp roles are the same as the forward kernel: 0-3 epilogue, 4-7 cp.async
-// producers, 8-11 index loaders, 12 TMEM allocator + tcgen05.mma issuer.
+// Warp roles are the same as the forward kernel: 0-3 epilogue, 4-11 cp.async
+// producers, 12-15 index loaders, 16 TMEM allocator + tcgen05.mma issuer.
 #include "kernels.h"
 
 namespace scb {
 namespace {
 
-constexpr int kThreads = 416;
+constexpr int kThreads = 544;
+constexpr int kEpiWarps = 4;     // warps 0-3
+constexpr int kProdWarp0 = 4;    // warps 4-11
+constexpr int kProdWarps = 8;
+constexpr int kLoadWarp0 = 12;   // warps 12-15
+constexpr int kMmaWarp = 16;
 constexpr int kIdxStages = 3;
 constexpr int kRows = 64;  // reduction rows per stage
 
@@ -103,7 +108,7 @@ __device__ __forceinline__ uint32_t tile_filter_bits(const WParams &P, int t) {
 }
 
 template <int kLag>
-__global__ void __maxnreg__(152) conv_wgrad_kernel(const __grid_constant__ WParams P) {
+__global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParams P) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_u32 = smem_u32(smem_raw);
   const uint32_t pad = (1024u - (raw_u32 & 1023u)) & 1023u;
@@ -133,12 +138,12 @@ __global__ void __maxnreg__(152) conv_wgrad_kernel(const __grid_constant__ WPara
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < S; ++i) {
-      mbar_init(&full_bar[i], 128);
+      mbar_init(&full_bar[i], kProdWarps * 32);
       mbar_init(&empty_bar[i], 1);
     }
     for (int i = 0; i < kIdxStages; ++i) {
       mbar_init(&idx_full[i], 128);
-      mbar_init(&idx_empty[i], 129);
+      mbar_init(&idx_empty[i], kProdWarps + 1);
     }
     mbar_init(acc_full, 1);
     mbar_init(drain_bar, 1);
@@ -146,7 +151,7 @@ __global__ void __maxnreg__(152) conv_wgrad_kernel(const __grid_constant__ WPara
     *used_tiles = 0;
     fence_mbar_init();
   }
-  if (warp == 12) {
+  if (warp == kMmaWarp) {
     tmem_alloc(tmem_slot, P.tmem_cols);
     tmem_relinquish();
   }
@@ -155,9 +160,9 @@ __global__ void __maxnreg__(152) conv_wgrad_kernel(const __grid_constant__ WPara
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  if (warp >= 8 && warp < 12) {
+  if (warp >= kLoadWarp0 && warp < kLoadWarp0 + 4) {
     // ---------------------------------------------------------------- index loaders
-    const int t = threadIdx.x - 256;
+    const int t = threadIdx.x - kLoadWarp0 * 32;
     const int r = t & 63;       // row of the chunk
     const int half = t >> 6;    // filter parity handled by this thread
     int it = 0;
@@ -247,33 +252,27 @@ __global__ void __maxnreg__(152) conv_wgrad_kernel(const __grid_constant__ WPara
       // loader threads passed the named barrier of this chunk
       mbar_arrive(&idx_full[b]);
     }
-  } else if (warp >= 4 && warp < 8) {
+  } else if (warp >= kProdWarp0 && warp < kProdWarp0 + kProdWarps) {
     // ---------------------------------------------------------------- producers
-    const int pt = threadIdx.x - 128;
+    // 256 threads; thread pt owns 16-byte unit u of rows rg + 32 i (i < 2) of
+    // every atom; gathered rows with a pair use cp.async, the others are
+    // zero-filled cp.async (src-size 0, no memory request).
+    const int pt = threadIdx.x - kProdWarp0 * 32;
     const int u = pt & 7;
-    const int rg = pt >> 3;  // 0..15
+    const int rg = pt >> 3;  // 0..31
     int it = 0;
     int64_t stage_ctr = 0;
-    int outstanding = 0;
     bool ok = true;
-    auto drain = [&]() {
-      cp_async_wait_all();
-      fence_proxy_async_smem();
-      while (outstanding > 0) {
-        mbar_arrive(&full_bar[(stage_ctr - outstanding) % S]);
-        --outstanding;
-      }
-    };
     const int n_b_atoms = P.n_mma / 64;
     for (int c = c_begin; c < c_end && ok; ++c, ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
-      if (!mbar_try_wait(&idx_full[b], ph)) {
-        drain();
-        if (!mbar_wait(&idx_full[b], ph, abort_flag)) {
-          flag_error(A.err, kErrWaitTimeout);
-          break;
-        }
+      int w_ok = 1;
+      if (lane == 0) w_ok = mbar_wait(&idx_full[b], ph, abort_flag) ? 1 : 0;
+      w_ok = __shfl_sync(0xffffffffu, w_ok, 0);
+      if (!w_ok) {
+        if (lane == 0) flag_error(A.err, kErrWaitTimeout);
+        break;
       }
       const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
       const int *tab = reinterpret_cast<const int *>(buf);
@@ -286,14 +285,17 @@ __global__ void __maxnreg__(152) conv_wgrad_kernel(const __grid_constant__ WPara
         const int tt = t0 + j;
         const int s = static_cast<int>(stage_ctr % S);
         const uint32_t eph = static_cast<uint32_t>((stage_ctr / S) & 1);
-        if (!mbar_wait(&empty_bar[s], eph ^ 1, abort_flag)) {
-          flag_error(A.err, kErrWaitTimeout);
+        int e_ok = 1;
+        if (lane == 0) e_ok = mbar_wait(&empty_bar[s], eph ^ 1, abort_flag) ? 1 : 0;
+        e_ok = __shfl_sync(0xffffffffu, e_ok, 0);
+        if (!e_ok) {
+          if (lane == 0) flag_error(A.err, kErrWaitTimeout);
           ok = false;
           break;
         }
         const uint32_t sA = smem_base + s * P.stage_bytes;
         const uint32_t sB = sA + P.b_off;
-        // M side: two atoms x 64 rows; unit u of rows rg + 16 i
+        // M side: two atoms x 64 rows
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int a = 2 * tt + h;
@@ -307,42 +309,42 @@ __global__ void __maxnreg__(152) conv_wgrad_kernel(const __grid_constant__ WPara
           }
           const bool atom_ok = a < P.n_atoms && k < A.kv;
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const int r = rg + 16 * i;
+          for (int i = 0; i < 2; ++i) {
+            const int r = rg + 32 * i;
             const int idx = atom_ok ? tab[(k - k_lo) * kRows + r] : -1;
-            const uint8_t *src =
-                A.input + (idx >= 0 ? static_cast<int64_t>(idx) * A.in_ld * 2 + byte0 : 0);
-            cp_async_16(sA + h * 8192 + sw128(r, u), src, idx >= 0 ? 16u : 0u);
+            const uint32_t dst = sA + h * 8192 + sw128(r, u);
+            if (idx >= 0) {
+              cp_async_16(dst, A.input + static_cast<int64_t>(idx) * A.in_ld * 2 + byte0, 16u);
+            } else {
+              cp_async_16(dst, A.input, 0u);  // zero fill, no memory request
+            }
           }
         }
         // N side: n_b_atoms atoms x 64 rows of dOut[sigma(r)]
         for (int na = 0; na < n_b_atoms; ++na) {
           const bool col_ok = na * 64 + u * 8 < A.K;
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const int r = rg + 16 * i;
+          for (int i = 0; i < 2; ++i) {
+            const int r = rg + 32 * i;
             const int sg = sig_tab[r];
-            const bool v = col_ok && sg >= 0;
-            const uint8_t *src =
-                A.dout + (v ? static_cast<int64_t>(sg) * A.dout_ld * 2 + na * 128 + u * 16 : 0);
-            cp_async_16(sB + na * 8192 + sw128(r, u), src, v ? 16u : 0u);
+            const uint32_t dst = sB + na * 8192 + sw128(r, u);
+            if (col_ok && sg >= 0) {
+              cp_async_16(dst, A.dout + static_cast<int64_t>(sg) * A.dout_ld * 2 + na * 128 + u * 16,
+                          16u);
+            } else {
+              cp_async_16(dst, A.dout, 0u);  // zero fill, no memory request
+            }
           }
         }
-        cp_async_commit();
+        cp_async_mbar_arrive_noinc(&full_bar[s]);
         ++stage_ctr;
-        ++outstanding;
-        if (outstanding > kLag) {
-          cp_async_wait<kLag>();
-          fence_proxy_async_smem();
-          mbar_arrive(&full_bar[(stage_ctr - outstanding) % S]);
-          --outstanding;
-        }
       }
       if (!ok) break;
-      mbar_arrive(&idx_empty[b]);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&idx_empty[b]);
     }
-    drain();
-  } else if (warp == 12) {
+    cp_async_wait_all();
+  } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
       int it = 0;
@@ -370,6 +372,7 @@ __global__ void __maxnreg__(152) conv_wgrad_kernel(const __grid_constant__ WPara
             ok = false;
             break;
           }
+          fence_proxy_async_smem();  // landed cp.async data -> tcgen05 operand reads
           tc_fence_after();
           const uint32_t sA = smem_base + s * P.stage_bytes;
           const uint32_t sB = sA + P.b_off;
@@ -400,7 +403,7 @@ __global__ void __maxnreg__(152) conv_wgrad_kernel(const __grid_constant__ WPara
       tc_fence_before();
       mbar_arrive(acc_full);  // release: used_tiles and the finished accumulators
     }
-  } else {
+  } else if (warp < kEpiWarps) {
     // ---------------------------------------------------------------- epilogue (warps 0-3)
     if (mbar_wait(acc_full, 0, abort_flag)) {
       tc_fence_after();
@@ -434,7 +437,7 @@ __global__ void __maxnreg__(152) conv_wgrad_kernel(const __grid_constant__ WPara
 
   tc_fence_before();
   __syncthreads();
-  if (warp == 12) {
+  if (warp == kMmaWarp) {
     __syncwarp();
     tc_fence_after();
     tmem_dealloc(tmem_base, P.tmem_cols);
@@ -518,7 +521,7 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t 
   uint32_t cols = 32;
   while (cols < static_cast<uint32_t>(per_group * P.n_mma)) cols <<= 1;
   P.tmem_cols = cols;
-  P.idesc = make_idesc(128, P.n_mma, 1u, true, true);  // bf16 only (checked by the caller)
+  P.idesc = make_idesc(128, P.n_mma, a.in_dtype == 12 ? 1u : 0u, true, true);
   int lag = stages - 2;
   if (lag > 4) lag = 4;
   if (lag < 1) lag = 1;

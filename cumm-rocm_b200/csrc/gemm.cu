@@ -275,6 +275,7 @@ cudaError_t launch_gemm(const GemmArgs &a, int num_sms, cudaStream_t s) {
   w.indices = nullptr;
   w.b_inds = a.shuffle == 2 ? a.b_inds : nullptr;
   w.ws = acc;
+  w.in_dtype = a.in_dtype;
   w.err = a.err;
   e = launch_conv_wgrad(w, num_sms, s);
   if (e != cudaSuccess) return e;

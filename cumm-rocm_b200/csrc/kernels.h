@@ -8,6 +8,12 @@
 
 namespace scb {
 
+// Encodes a 2-D SWIZZLE_128B TMA tensor map over a row-major [outer, inner]
+// tensor (row stride in bytes) with a box of box_outer rows x 128 bytes.
+// Returns false when TMA cannot describe the tensor (alignment, sizes).
+bool encode_tmap_2d(void *out_map, int dtype, const void *base, uint64_t inner, uint64_t outer,
+                    uint64_t row_stride_bytes, uint32_t box_inner, uint32_t box_outer);
+
 // ------------------------------------------------------------------ conv fwd / dgrad (tcgen05)
 // Row-gather implicit GEMM: for every 128-row tile of the sorted row order,
 //   out[sigma(r), n] = epi( sum_{k in tile mask} sum_c A[idx[k][sigma(r)], c] * B[n, k, c] )
@@ -72,6 +78,7 @@ struct ConvWgradArgs {
   const int32_t *argsort;
   const int32_t *indices;
   float *ws;                 // [K, kv, C] fp32, zeroed
+  int in_dtype;              // 12 bf16 or 7 f16 (dOut and input)
   int *err;
   // ShuffleAB GEMM mode (indices == nullptr, kv == 1): input row of sorted row r
   // is b_inds ? b_inds[r] : r; dOut row is argsort ? argsort[r] : r; mask may be null

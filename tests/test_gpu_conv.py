@@ -195,11 +195,21 @@ def test_edge_cases():
     dd = find_desp(ConvOpType.kBackwardInput, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 128)
     conv(ConvOpType.kBackwardInput, dd, din, w, out, pf, m, order, reverse_mask=True)
     assert torch.all(din == 3.0)
-    # N = 0
+    # N = 0: an empty index table is rejected like the reference prologue
+    # (TV_ASSERT_RT_ERR(!indices.empty()), cumm/conv/nvrtc_code.py:123-125)
     e = torch.zeros((0, C), dtype=torch.bfloat16, device="cuda")
     eo = torch.zeros((0, K), dtype=torch.bfloat16, device="cuda")
-    conv(ConvOpType.kForward, desp, e, w, eo, np.zeros((27, 0), np.int32), np.zeros(0, np.uint32),
-         np.zeros(0, np.int32))
+    with pytest.raises(RuntimeError, match="indices"):
+        conv(ConvOpType.kForward, desp, e, w, eo, np.zeros((27, 0), np.int32),
+             np.zeros(0, np.uint32), np.zeros(0, np.int32))
+    # ragged: N not a multiple of the tile, one row
+    pf1 = np.full((27, 1), -1, np.int32)
+    pf1[13, 0] = 0
+    x1 = dev(np.full((1, C), 2.0, np.float32), torch.bfloat16)
+    o1 = torch.zeros((1, K), dtype=torch.bfloat16, device="cuda")
+    conv(ConvOpType.kForward, desp, x1, w, o1, pf1, np.array([1 << 13], np.uint32),
+         np.zeros(1, np.int32))
+    assert torch.all(o1.float() == 2.0 * C)
 
 
 def test_bad_index_reported():

@@ -51,7 +51,13 @@ def test_dense(dt, dc, ta, tb, m, n, k):
     at, bt = _t(a, dt), _t(b, dt)
     c = torch.zeros((m, n), dtype=dc, device="cuda")
     tvd = {torch.bfloat16: tv.bfloat16, torch.float16: tv.float16, torch.float32: tv.float32}
-    _run(_desp("Tcgen05", tvd[dt], tvd[dc], ta, tb, ShuffleStrideType.kNoShuffle), at, bt, c)
+    desp = _desp("Tcgen05", tvd[dt], tvd[dc], ta, tb, ShuffleStrideType.kNoShuffle)
+    if not desp.supported(m, n, k):
+        # misaligned contiguous dimension: rejected like the reference prologue
+        with pytest.raises(ValueError, match="misaligned"):
+            _run(desp, at, bt, c)
+        return
+    _run(desp, at, bt, c)
     ref = co.gemm(_f64(at), _f64(bt), ta, tb)
     nr, _, _ = co.rel_err(_f64(c), ref)
     assert nr < 2e-3
