@@ -207,6 +207,8 @@ def run_b200(args, rank, world, dist):
             p.mask = tv.Tensor(mo_, tv.uint32)
             p.mask_width = 128
         p.mask_argsort = tv.Tensor(pt_.argsorts_fwd[0])
+        p.indices_sorted = tv.Tensor(pt_.sorted_indices(
+            "bwd" if op == ConvOpType.kBackwardInput else "fwd"))
         p.stream = sptr
         cp, _ = build_conv_params_c(p)
         need = ctypes.c_int64(0)
@@ -307,6 +309,8 @@ def run_b200(args, rank, world, dist):
                 p.mask = tv.Tensor(mod, tv.uint32)
                 p.mask_width = 128
             p.mask_argsort = tv.Tensor(ptd.argsorts_fwd[0])
+            p.indices_sorted = tv.Tensor(ptd.sorted_indices(
+                "bwd" if op == ConvOpType.kBackwardInput else "fwd"))
             p.stream = sptr
             cmt.implicit_gemm2(p)
         out_h.copy_(outd, non_blocking=True)

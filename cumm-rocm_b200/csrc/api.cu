@@ -369,6 +369,7 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     a.argsort = p->mask_argsort;
     a.indices = p->indices;
     a.a_inds = nullptr;
+    a.idx_sorted = p->indices_sorted;
     a.mask_out = fwd ? p->mask_output : nullptr;
     a.tile_m_desp = p->tile_m;
     a.mask_filter = p->mask_filter;
@@ -407,6 +408,7 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     a.ws = static_cast<float *>(p->workspace);
     a.err = err;
     a.b_inds = nullptr;
+    a.idx_sorted = p->indices_sorted;
     a.in_dtype = p->dtype_input;
     e = scb::launch_conv_wgrad(a, sms, s);
     if (e != cudaSuccess) return cuda_fail(e, "conv wgrad launch");
@@ -611,6 +613,18 @@ int sc_build_conv_pairs(const int32_t *coords, int64_t n_in, int32_t batch, cons
                                         mask_bwd, workspace, workspace_bytes,
                                         static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "build_conv_pairs");
+  return SC_OK;
+}
+
+int sc_sort_indices(const int32_t *indices, int32_t kv, int64_t N, const int32_t *argsort,
+                    int32_t *indices_sorted, void *stream) {
+  g_last_error.clear();
+  if (N > 0 && (indices == nullptr || argsort == nullptr || indices_sorted == nullptr))
+    return fail(SC_INVALID_ARG, "null indices / argsort / output");
+  if (kv < 1 || kv > 32 || N < 0) return fail(SC_INVALID_ARG, "bad kv / N");
+  cudaError_t e = scb::sort_indices(indices, kv, N, argsort, indices_sorted,
+                                    static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "sort_indices");
   return SC_OK;
 }
 

@@ -166,7 +166,6 @@ constexpr int kProdWarp0 = 4;    // warps 4-11
 constexpr int kProdWarps = 8;
 constexpr int kLoadWarp0 = 12;   // warps 12-15
 constexpr int kMmaWarp = 16;
-constexpr int kProdThreads = kProdWarps * 32;
 
 template <bool kF8, typename TOut, bool kTma>
 __global__ void __maxnreg__(96)
@@ -195,14 +194,14 @@ __global__ void __maxnreg__(96)
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < S; ++i) {
-      // every producer thread arrives through cp.async.mbarrier.arrive.noinc;
-      // with the TMA weight load one more arrive.expect_tx
-      mbar_init(&full_bar[i], kProdThreads + (kTma ? 1 : 0));
+      // the 32 lanes of the stage's producer warp arrive through
+      // cp.async.mbarrier.arrive.noinc; with TMA one more arrive.expect_tx
+      mbar_init(&full_bar[i], 32 + (kTma ? 1 : 0));
       mbar_init(&empty_bar[i], 1);
     }
     for (int i = 0; i < kIdxStages; ++i) {
       mbar_init(&idx_full[i], 128);
-      mbar_init(&idx_empty[i], kProdWarps + 1);
+      mbar_init(&idx_empty[i], min(S, kProdWarps) + 1);
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(&acc_full[i], 1);
@@ -226,7 +225,7 @@ __global__ void __maxnreg__(96)
     const int r = threadIdx.x - kLoadWarp0 * 32;  // row inside the tile
     const int lw = r >> 5;
     int it = 0;
-    for (int64_t tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
+    for (int tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
       if (!mbar_wait(&idx_empty[b], ph ^ 1, abort_flag)) {
@@ -292,7 +291,9 @@ __global__ void __maxnreg__(96)
           const int k = kb + q;
           int v = -1;
           if (k < A.kv && ((tm >> k) & 1u) && sig >= 0 && ((sub >> k) & 1u)) {
-            if (A.indices)
+            if (A.idx_sorted)  // coalesced: row_g is the sorted row
+              v = __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.M + row_g);
+            else if (A.indices)
               v = __ldg(A.indices + static_cast<int64_t>(k) * A.M + sig);
             else
               v = A.a_inds ? __ldg(A.a_inds + row_g) : static_cast<int>(row_g);
@@ -330,20 +331,26 @@ __global__ void __maxnreg__(96)
     }
   } else if (warp >= kProdWarp0 && warp < kProdWarp0 + kProdWarps) {
     // ---------------------------------------------------------------- producers
-    // 256 threads; thread pt owns 16-byte unit u of rows rg + 32 i (i < 4).
+    // Producer warp pw owns shared-memory stage pw (S <= kProdWarps stages;
+    // warps beyond S stay idle) and fills every chunk c with c % S == pw
+    // alone: lane owns 16-byte unit u of rows rg + 4 i (i < 32).  The S stages
+    // are filled concurrently and the per-stage synchronisation is amortised
+    // over 32 copies per lane.  One owner per stage also keeps every empty-
+    // barrier wait exactly one phase ahead of the MMA warp (a parity wait
+    // cannot tell phase k from k + 2).
     // Rows with a pair are fetched with 16-byte cp.async; rows without one are
     // zero-filled cp.async (src-size 0, no memory request).  With TMA the
-    // weight slab is one 2-D tiled load issued by thread 0.
-    const int pt = threadIdx.x - kProdWarp0 * 32;
-    const int u = pt & 7;
-    const int rg = pt >> 3;
+    // weight slab is one 2-D tiled load issued by lane 0.
+    const int pw = warp - kProdWarp0;
+    const int u = lane & 7;
+    const int rg = lane >> 3;
     const int esz = kF8 ? 1 : 2;
     const int box = 128 / esz;
     const uint32_t b_tx = static_cast<uint32_t>(A.BN) * 128;
     int it = 0;
-    int64_t chunk_ctr = 0;
-    bool ok = true;
-    for (int64_t tile = blockIdx.x; tile < P.num_tiles && ok; tile += gridDim.x, ++it) {
+    uint32_t c_base = 0;  // chunks of all previous tiles
+    bool ok = pw < S;
+    for (int tile = blockIdx.x; tile < P.num_tiles && ok; tile += gridDim.x, ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
       int w_ok = 1;
@@ -358,57 +365,70 @@ __global__ void __maxnreg__(96)
       const Meta *meta = reinterpret_cast<const Meta *>(buf + A.kv * kTileM * 4);
       const int nch = meta->nchunks;
       const int na = meta->n_active;
-      const int n0 = static_cast<int>(tile % A.n_tiles) * A.BN;
-      for (int j = 0; j < nch; ++j) {
-        const int s = static_cast<int>(chunk_ctr % S);
-        const uint32_t eph = static_cast<uint32_t>((chunk_ctr / S) & 1);
+      const int n0 = (tile % A.n_tiles) * A.BN;
+      const uint32_t uS = static_cast<uint32_t>(S);
+      const int j0 = static_cast<int>((static_cast<uint32_t>(pw) + uS - c_base % uS) % uS);
+      for (int j = j0; j < nch; j += S) {
+        const uint32_t c = c_base + static_cast<uint32_t>(j);
+        const uint32_t s = static_cast<uint32_t>(pw);  // == c % S
+        const uint32_t eph = (c / uS) & 1u;
+        int slot_a, cb;
+        if (P.cpo > 0) {
+          slot_a = j / P.cpo;
+          cb = j - slot_a * P.cpo;
+        } else {
+          slot_a = 0;
+          cb = 0;
+        }
         int e_ok = 1;
-        if (lane == 0) e_ok = mbar_wait(&empty_bar[s], eph ^ 1, abort_flag) ? 1 : 0;
+        const uint32_t sA = smem_base + s * P.stage_bytes;
+        const uint32_t sB = sA + P.b_off;
+        if (lane == 0) {
+          e_ok = mbar_wait(&empty_bar[s], eph ^ 1, abort_flag) ? 1 : 0;
+          if constexpr (kTma) {
+            if (e_ok) {
+              mbar_arrive_expect_tx(&full_bar[s], b_tx);
+              const int xb = meta->k_list[slot_a] * (A.b_off_stride / esz) + cb * box;
+              tma_load_2d(sB, &P.tmap_b, xb, n0, &full_bar[s]);
+            }
+          }
+        }
         e_ok = __shfl_sync(0xffffffffu, e_ok, 0);
         if (!e_ok) {
           if (lane == 0) flag_error(A.err, kErrWaitTimeout);
           ok = false;
           break;
         }
-        const uint32_t sA = smem_base + s * P.stage_bytes;
-        const uint32_t sB = sA + P.b_off;
         int slot, byte0;
         if (P.cpo > 0) {
-          slot = j / P.cpo;
-          byte0 = (j % P.cpo) * 128 + u * 16;
+          slot = slot_a;
+          byte0 = cb * 128 + u * 16;
         } else {
           slot = j * P.opc + u / P.upo;
           byte0 = (u % P.upo) * 16;
         }
-        if constexpr (kTma) {
-          if (pt == 0) {
-            mbar_arrive_expect_tx(&full_bar[s], b_tx);
-            const int cb = j % P.cpo;
-            const int xb = meta->k_list[slot] * (A.b_off_stride / esz) + cb * box;
-            tma_load_2d(sB, &P.tmap_b, xb, n0, &full_bar[s]);
-          }
-        }
         const bool slot_ok = slot < na && byte0 < A.a_row_bytes;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int r = rg + 32 * i;
-          const int idx = slot_ok ? tab[slot * kTileM + r] : -1;
+        const int *trow = tab + slot * kTileM;
+        const uint8_t *abase = A.a_base + byte0;
+#pragma unroll 8
+        for (int i = 0; i < kTileM / 4; ++i) {
+          const int r = rg + 4 * i;
+          const int idx = slot_ok ? trow[r] : -1;
           const uint32_t dst = sA + sw128(r, u);
-          if (idx >= 0) {
-            cp_async_16(dst, A.a_base + static_cast<int64_t>(idx) * A.a_row_stride + byte0, 16u);
-          } else {
+          if (idx >= 0)
+            cp_async_16(dst, abase + static_cast<int64_t>(idx) * A.a_row_stride, 16u);
+          else
             cp_async_16(dst, A.a_base, 0u);  // zero fill, no memory request
-          }
         }
         if constexpr (!kTma) {
-          // B: BN rows x 8 units over the 256 producer threads
-          for (int q = pt; q < A.BN * 8; q += kProdThreads) {
+          // B: BN rows x 8 units over the warp's 32 lanes
+          for (int q = lane; q < A.BN * 8; q += 32) {
             const int n = q >> 3;
             const int uu = q & 7;
             int kb, bbyte;
             if (P.cpo > 0) {
               kb = meta->k_list[slot];
-              bbyte = (j % P.cpo) * 128 + uu * 16;
+              bbyte = cb * 128 + uu * 16;
             } else {
               const int sl = j * P.opc + uu / P.upo;
               kb = sl < na ? meta->k_list[sl] : -1;
@@ -426,11 +446,11 @@ __global__ void __maxnreg__(96)
             }
           }
         }
-        // the stage's full barrier counts this thread once its copies land
+        // the stage's full barrier counts each lane once its copies land
         cp_async_mbar_arrive_noinc(&full_bar[s]);
-        ++chunk_ctr;
       }
       if (!ok) break;
+      c_base += static_cast<uint32_t>(nch);
       __syncwarp();
       if (lane == 0) mbar_arrive(&idx_empty[b]);
     }
@@ -439,9 +459,10 @@ __global__ void __maxnreg__(96)
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
       int it = 0;
-      int64_t chunk_ctr = 0;
+      uint32_t stage = 0, fph = 0;
       bool issued = false;
-      for (int64_t tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
+      const uint64_t a_desc0 = make_sdesc(smem_base, 16, 1024);
+      for (int tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
         const int b = it % kIdxStages;
         const uint32_t ph = (it / kIdxStages) & 1;
         if (!mbar_wait(&idx_full[b], ph, abort_flag)) {
@@ -466,20 +487,20 @@ __global__ void __maxnreg__(96)
         }
         bool ok = true;
         for (int j = 0; j < nch; ++j) {
-          const int s = static_cast<int>(chunk_ctr % S);
-          const uint32_t fph = static_cast<uint32_t>((chunk_ctr / S) & 1);
+          const uint32_t s = stage;
           if (!mbar_wait(&full_bar[s], fph, abort_flag)) {
             flag_error(A.err, kErrWaitTimeout);
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t sA = smem_base + s * P.stage_bytes;
-          const uint32_t sB = sA + P.b_off;
+          const uint64_t ad0 = a_desc0 + static_cast<uint64_t>((s * P.stage_bytes) >> 4);
+          const uint64_t bd0 = ad0 + static_cast<uint64_t>(P.b_off >> 4);
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk) {
-            const uint64_t ad = make_sdesc(sA + kk * 32, 16, 1024);
-            const uint64_t bd = make_sdesc(sB + kk * 32, 16, 1024);
+            // K advances 32 bytes inside the SWIZZLE_128B atom (start address >> 4)
+            const uint64_t ad = ad0 + static_cast<uint64_t>(kk * 2);
+            const uint64_t bd = bd0 + static_cast<uint64_t>(kk * 2);
             if constexpr (kF8)
               mma_f8(d, ad, bd, P.idesc, (j | kk) != 0 ? 1u : 0u);
             else
@@ -487,7 +508,10 @@ __global__ void __maxnreg__(96)
           }
           issued = true;
           mma_commit(&empty_bar[s]);
-          ++chunk_ctr;
+          if (++stage == static_cast<uint32_t>(S)) {
+            stage = 0;
+            fph ^= 1u;
+          }
         }
         if (!ok) break;
         mma_commit(&acc_full[ab]);
@@ -505,7 +529,7 @@ __global__ void __maxnreg__(96)
     const int r = threadIdx.x;  // TMEM lane == tile row
     int it = 0;
     const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
-    for (int64_t tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
+    for (int tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
       const int64_t tile_m = tile / A.n_tiles;
       const int n0 = static_cast<int>(tile % A.n_tiles) * A.BN;
       const int64_t row_g = tile_m * kTileM + r;

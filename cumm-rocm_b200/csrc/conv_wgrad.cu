@@ -138,12 +138,12 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < S; ++i) {
-      mbar_init(&full_bar[i], kProdWarps * 32);
+      mbar_init(&full_bar[i], 32);
       mbar_init(&empty_bar[i], 1);
     }
     for (int i = 0; i < kIdxStages; ++i) {
       mbar_init(&idx_full[i], 128);
-      mbar_init(&idx_empty[i], kProdWarps + 1);
+      mbar_init(&idx_empty[i], min(S, kProdWarps) + 1);
     }
     mbar_init(acc_full, 1);
     mbar_init(drain_bar, 1);
@@ -222,7 +222,9 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
         const int k = k_lo + 2 * q + half;
         int v = -1;
         if (k < k_hi && ((word >> k) & 1u) && sig >= 0) {
-          if (A.indices)
+          if (A.idx_sorted)  // coalesced: row is the sorted row
+            v = __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.N + row);
+          else if (A.indices)
             v = __ldg(A.indices + static_cast<int64_t>(k) * A.N + sig);
           else
             v = A.b_inds ? __ldg(A.b_inds + row) : static_cast<int>(row);
@@ -254,15 +256,20 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
     }
   } else if (warp >= kProdWarp0 && warp < kProdWarp0 + kProdWarps) {
     // ---------------------------------------------------------------- producers
-    // 256 threads; thread pt owns 16-byte unit u of rows rg + 32 i (i < 2) of
-    // every atom; gathered rows with a pair use cp.async, the others are
-    // zero-filled cp.async (src-size 0, no memory request).
-    const int pt = threadIdx.x - kProdWarp0 * 32;
-    const int u = pt & 7;
-    const int rg = pt >> 3;  // 0..31
+    // Producer warp pw owns shared-memory stage pw (S <= kProdWarps; warps
+    // beyond S stay idle) and fills every stage index g with g % S == pw
+    // alone: lane owns 16-byte unit u of rows rg + 4 i (i < 16) of every
+    // atom.  One owner per stage keeps each empty-barrier wait exactly one
+    // phase ahead of the MMA warp.
+    // Gathered rows with a pair use cp.async, the others are zero-filled
+    // cp.async (src-size 0, no memory request).
+    const int pw = warp - kProdWarp0;
+    const int u = lane & 7;
+    const int rg = lane >> 3;
     int it = 0;
-    int64_t stage_ctr = 0;
-    bool ok = true;
+    uint32_t st_base = 0;  // stages of all previous chunks
+    bool ok = pw < S;
+    const uint32_t uS = static_cast<uint32_t>(S);
     const int n_b_atoms = P.n_mma / 64;
     for (int c = c_begin; c < c_end && ok; ++c, ++it) {
       const int b = it % kIdxStages;
@@ -279,12 +286,16 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       const int *sig_tab = tab + 32 * kRows;
       const WMeta *meta = reinterpret_cast<const WMeta *>(sig_tab + kRows);
       uint32_t bits = meta->active_bits;
+      uint32_t local = 0;  // index of the stage inside this chunk
       while (bits) {
-        const int j = __ffs(bits) - 1;
+        const int jt = __ffs(bits) - 1;
         bits &= bits - 1;
-        const int tt = t0 + j;
-        const int s = static_cast<int>(stage_ctr % S);
-        const uint32_t eph = static_cast<uint32_t>((stage_ctr / S) & 1);
+        const uint32_t g_stage = st_base + local;
+        ++local;
+        if (g_stage % uS != static_cast<uint32_t>(pw)) continue;
+        const int tt = t0 + jt;
+        const uint32_t s = static_cast<uint32_t>(pw);  // == g_stage % S
+        const uint32_t eph = (g_stage / uS) & 1u;
         int e_ok = 1;
         if (lane == 0) e_ok = mbar_wait(&empty_bar[s], eph ^ 1, abort_flag) ? 1 : 0;
         e_ok = __shfl_sync(0xffffffffu, e_ok, 0);
@@ -308,38 +319,37 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
             byte0 = (u % P.upf) * 16;
           }
           const bool atom_ok = a < P.n_atoms && k < A.kv;
-#pragma unroll
-          for (int i = 0; i < 2; ++i) {
-            const int r = rg + 32 * i;
-            const int idx = atom_ok ? tab[(k - k_lo) * kRows + r] : -1;
+          const int *trow = tab + (k - k_lo) * kRows;
+#pragma unroll 4
+          for (int i = 0; i < kRows / 4; ++i) {
+            const int r = rg + 4 * i;
+            const int idx = atom_ok ? trow[r] : -1;
             const uint32_t dst = sA + h * 8192 + sw128(r, u);
-            if (idx >= 0) {
+            if (idx >= 0)
               cp_async_16(dst, A.input + static_cast<int64_t>(idx) * A.in_ld * 2 + byte0, 16u);
-            } else {
+            else
               cp_async_16(dst, A.input, 0u);  // zero fill, no memory request
-            }
           }
         }
         // N side: n_b_atoms atoms x 64 rows of dOut[sigma(r)]
         for (int na = 0; na < n_b_atoms; ++na) {
           const bool col_ok = na * 64 + u * 8 < A.K;
-#pragma unroll
-          for (int i = 0; i < 2; ++i) {
-            const int r = rg + 32 * i;
+#pragma unroll 4
+          for (int i = 0; i < kRows / 4; ++i) {
+            const int r = rg + 4 * i;
             const int sg = sig_tab[r];
             const uint32_t dst = sB + na * 8192 + sw128(r, u);
-            if (col_ok && sg >= 0) {
+            if (col_ok && sg >= 0)
               cp_async_16(dst, A.dout + static_cast<int64_t>(sg) * A.dout_ld * 2 + na * 128 + u * 16,
                           16u);
-            } else {
+            else
               cp_async_16(dst, A.dout, 0u);  // zero fill, no memory request
-            }
           }
         }
         cp_async_mbar_arrive_noinc(&full_bar[s]);
-        ++stage_ctr;
       }
       if (!ok) break;
+      st_base += local;
       __syncwarp();
       if (lane == 0) mbar_arrive(&idx_empty[b]);
     }
@@ -348,7 +358,7 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
       int it = 0;
-      int64_t stage_ctr = 0;
+      uint32_t stage = 0, fph = 0;
       uint32_t started = 0;
       bool ok = true;
       for (int c = c_begin; c < c_end && ok; ++c, ++it) {
@@ -365,14 +375,12 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
         while (bits) {
           const int j = __ffs(bits) - 1;
           bits &= bits - 1;
-          const int s = static_cast<int>(stage_ctr % S);
-          const uint32_t fph = static_cast<uint32_t>((stage_ctr / S) & 1);
+          const uint32_t s = stage;
           if (!mbar_wait(&full_bar[s], fph, abort_flag)) {
             flag_error(A.err, kErrWaitTimeout);
             ok = false;
             break;
           }
-          fence_proxy_async_smem();  // landed cp.async data -> tcgen05 operand reads
           tc_fence_after();
           const uint32_t sA = smem_base + s * P.stage_bytes;
           const uint32_t sB = sA + P.b_off;
@@ -386,7 +394,10 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
           }
           started |= 1u << j;
           mma_commit(&empty_bar[s]);
-          ++stage_ctr;
+          if (++stage == static_cast<uint32_t>(S)) {
+            stage = 0;
+            fph ^= 1u;
+          }
         }
       }
       if (started) {

@@ -50,6 +50,7 @@ struct ConvRowGatherArgs {
   // A row of sorted row r = a_inds ? a_inds[r] : r, output row = argsort ? argsort[r] : r
   const int32_t *a_inds;
   int64_t out_rows;          // bound for output rows
+  const int32_t *idx_sorted; // optional [kv, M]: indices[k][argsort[r]]
 };
 cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaStream_t stream);
 
@@ -83,6 +84,7 @@ struct ConvWgradArgs {
   // ShuffleAB GEMM mode (indices == nullptr, kv == 1): input row of sorted row r
   // is b_inds ? b_inds[r] : r; dOut row is argsort ? argsort[r] : r; mask may be null
   const int32_t *b_inds;
+  const int32_t *idx_sorted; // optional [kv, N]: indices[k][argsort[r]]
 };
 cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t stream);
 
@@ -162,6 +164,8 @@ cudaError_t build_conv_pairs(const PairBuildArgs &a, int64_t n_out, int32_t *out
                              int32_t *pairs_fwd, int32_t *pairs_bwd, uint32_t *mask_fwd,
                              uint32_t *mask_bwd, void *ws, int64_t ws_bytes, cudaStream_t s);
 int64_t sort_workspace_bytes(int64_t n);
+cudaError_t sort_indices(const int32_t *indices, int kv, int64_t n, const int32_t *argsort,
+                         int32_t *out, cudaStream_t s);
 cudaError_t sort_masks_split(uint32_t *data, int64_t n, uint32_t split_mask, int32_t *argsort,
                              void *ws, int64_t ws_bytes, cudaStream_t s);
 

@@ -519,6 +519,27 @@ cudaError_t build_conv_pairs(const PairBuildArgs &a, int64_t n_out, int32_t *out
   return cudaGetLastError();
 }
 
+namespace {
+__global__ void sort_indices_kernel(const int32_t *indices, int kv, int64_t n,
+                                    const int32_t *argsort, int32_t *out, int *err) {
+  const int64_t total = static_cast<int64_t>(kv) * n;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t k = i / n, r = i % n;
+    const int sig = argsort[r];
+    out[i] = (sig >= 0 && sig < n) ? indices[k * n + sig] : -1;
+  }
+}
+}  // namespace
+
+cudaError_t sort_indices(const int32_t *indices, int kv, int64_t n, const int32_t *argsort,
+                         int32_t *out, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  sort_indices_kernel<<<grid_for(static_cast<int64_t>(kv) * n), kThreads, 0, s>>>(
+      indices, kv, n, argsort, out, nullptr);
+  return cudaGetLastError();
+}
+
 int64_t sort_workspace_bytes(int64_t n) { return align_up(n * 4) + radix_ws_bytes(n, 4); }
 
 cudaError_t sort_masks_split(uint32_t *data, int64_t n, uint32_t split_mask, int32_t *argsort,

@@ -20,7 +20,7 @@ EXPORTS = (
     "sc_conv_implicit_gemm", "sc_conv_workspace_size", "sc_gemm_matmul", "sc_gemm_workspace_size",
     "sc_pairs_workspace_size", "sc_build_subm_pairs", "sc_build_conv_outputs",
     "sc_build_conv_pairs", "sc_sort_masks_split", "sc_sort_workspace_size",
-    "sc_check_device_error", "sc_last_error", "sc_version",
+    "sc_check_device_error", "sc_last_error", "sc_version", "sc_sort_indices",
 )
 
 c_i32, c_i64, c_u32, c_f32, c_vp = (ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32,
@@ -39,6 +39,7 @@ class ConvParamsC(ctypes.Structure):
         ("act_alpha", c_f32), ("act_beta", c_f32), ("act_type", c_i32), ("bias", c_vp),
         ("output_add", c_vp), ("scale", c_vp), ("split_k_slices", c_i32), ("flags", c_i32),
         ("workspace", c_vp), ("workspace_bytes", c_i64), ("stream", c_vp),
+        ("indices_sorted", c_vp),
     ]
 
 
@@ -90,6 +91,7 @@ def load() -> ctypes.CDLL:
         lib.sc_sort_masks_split.argtypes = [c_vp, c_i64, c_u32, c_vp, c_vp, c_i64, c_vp]
         lib.sc_sort_workspace_size.argtypes = [c_i64, P(c_i64)]
         lib.sc_check_device_error.argtypes = [c_vp, P(c_i32)]
+        lib.sc_sort_indices.argtypes = [c_vp, c_i32, c_i64, c_vp, c_vp, c_vp]
         lib.sc_last_error.restype = ctypes.c_char_p
         lib.sc_version.restype = ctypes.c_char_p
         for name in EXPORTS:

@@ -139,6 +139,12 @@ def build_conv_params_c(params: ConvParams) -> Tuple[_lib.ConvParamsC, dict]:
     cp.split_k_slices = int(params.split_k_slices)
     cp.flags = 0
     cp.stream = int(params.stream) if params.stream else None
+    isorted = getattr(params, "indices_sorted", None)
+    if isorted is not None and not isorted.empty():
+        if list(isorted.shape) != list(params.indices.shape):
+            raise ValueError("indices_sorted must have the shape of indices")
+        _check_dense(isorted, "indices_sorted")
+        cp.indices_sorted = isorted.byte_pointer()
     return cp, {"kv": kv, "C": C, "K": K}
 
 

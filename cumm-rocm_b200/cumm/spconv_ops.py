@@ -157,6 +157,20 @@ class SpconvOps:
     def sort_1d_by_key(data, stream: int = 0):
         return SpconvOps.sort_1d_by_key_split(data, 0xffffffff, stream)
 
+    @staticmethod
+    def sort_indices(indices, argsort, stream: int = 0):
+        """indices [kv, N] permuted into argsort order: out[k][r] =
+        indices[k][argsort[r]] (the optional ConvParams.indices_sorted)."""
+        _lib.require_cuda()
+        lib = _lib.load()
+        ind, srt = _t(indices), _t(argsort)
+        kv, n = ind.shape
+        out = torch.empty_like(ind)
+        _lib.check(lib.sc_sort_indices(_vp(ind), kv, n, _vp(srt), _vp(out), _stream(stream)))
+        if isinstance(indices, tv.Tensor):
+            return tv.Tensor(out, tv.int32)
+        return out
+
 
 def _as_i32(v: int) -> int:
     v &= 0xffffffff
@@ -184,6 +198,22 @@ class PairTable:
     def pair_count(self) -> int:
         """P = number of valid (input, output) pairs."""
         return int((self.pairs_fwd >= 0).sum().item())
+
+    def sorted_indices(self, which: str = "fwd", split: int = 0) -> torch.Tensor:
+        """Index table of `which` ('fwd' or 'bwd') permuted into the argsort
+        order the matching convolution uses: forward and backward-weight walk
+        pairs_fwd in argsorts_fwd order; backward-input walks pairs_bwd in
+        argsorts_fwd order (submanifold, reverse_mask) or argsorts_bwd order
+        (strided).  Cached per (which, split)."""
+        cache = self.__dict__.setdefault("_sorted_cache", {})
+        key = (which, split)
+        if key not in cache:
+            if which == "fwd":
+                cache[key] = SpconvOps.sort_indices(self.pairs_fwd, self.argsorts_fwd[split])
+            else:
+                order = self.argsorts_fwd[split] if self.subm else self.argsorts_bwd[split]
+                cache[key] = SpconvOps.sort_indices(self.pairs_bwd, order)
+        return cache[key]
 
 
 def build_pair_table(coords: torch.Tensor, spatial_shape: Sequence[int], ksize=(3, 3, 3),

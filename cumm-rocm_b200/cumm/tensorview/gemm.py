@@ -404,3 +404,7 @@ class ConvParams:
         self.indices = Tensor()
         self.mask_output = Tensor()
         self.stream = 0
+        # extension (no counterpart in the reference): indices permuted into
+        # mask_argsort order (SpconvOps.sort_indices); lets the kernels read
+        # the index table coalesced; results are identical
+        self.indices_sorted = Tensor()

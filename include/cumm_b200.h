@@ -117,6 +117,12 @@ typedef struct sc_conv_params {
   void *workspace;
   int64_t workspace_bytes;
   void *stream; /* cudaStream_t */
+  /* Optional (may be NULL): indices permuted into mask_argsort order,
+   * indices_sorted[k][r] = indices[k][mask_argsort[r]] ([kv, N] int32), as
+   * produced by sc_sort_indices.  With it the kernels read the index table
+   * coalesced instead of through the argsort indirection; results are
+   * identical. */
+  const int32_t *indices_sorted;
 } sc_conv_params;
 
 /*
@@ -223,6 +229,12 @@ int sc_build_conv_pairs(const int32_t *coords, int64_t n_in, int32_t batch,
 int sc_sort_masks_split(uint32_t *data, int64_t n, uint32_t split_mask, int32_t *argsort,
                         void *workspace, int64_t workspace_bytes, void *stream);
 int sc_sort_workspace_size(int64_t n, int64_t *bytes);
+
+/* indices_sorted[k][r] = indices[k][argsort[r]] for k < kv, r < N (a gather
+ * kernel on `stream`; prepares sc_conv_params.indices_sorted for a pair table
+ * that is reused by several convolutions). */
+int sc_sort_indices(const int32_t *indices, int32_t kv, int64_t N, const int32_t *argsort,
+                    int32_t *indices_sorted, void *stream);
 
 /* Device error word of the current device: returns the accumulated error bits
  * (0 = none) after synchronising `stream`, and clears them. */

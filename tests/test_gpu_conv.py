@@ -258,3 +258,62 @@ def test_lidar_200k_fwd_dgrad_wgrad(seed):
          find_desp(ConvOpType.kBackwardWeight, "Tcgen05", tv.bfloat16, tv.float32, tv.bfloat16, 128),
          xt, dw, dyt, pf, mo.numpy(), order, mask_width=128)
     _assert_close(to64(dw), co.wgrad_gather_gemm_scatter(dy64, x64, pf), TOL_16)
+
+
+def test_sorted_index_table_identical():
+    """ConvParams.indices_sorted (coalesced index table) gives bit-identical
+    results for fwd, dgrad and wgrad."""
+    import torch as _t
+    from cumm.spconv_ops import build_pair_table
+    n, C, K = 30000, 64, 64
+    coords = vg.lidar_voxels(n, seed=5)
+    pt = build_pair_table(_t.from_numpy(coords).cuda(), vg.KITTI_SHAPE)
+    rng = np.random.default_rng(5)
+    x = dev(rng.standard_normal((n, C)).astype(np.float32), torch.bfloat16)
+    w = dev(vg.kaiming_uniform(K, 27, C, 5), torch.bfloat16)
+    dy = dev(rng.standard_normal((n, K)).astype(np.float32), torch.bfloat16)
+    m = pt.masks_fwd[0].cpu().numpy().view(np.uint32)
+    order = pt.argsorts_fwd[0].cpu().numpy()
+    from cumm.conv.main import ConvMainUnitTest
+    from cumm.tensorview.gemm import ConvParams
+    outs = []
+    for use_sorted in (False, True):
+        res = []
+        for op, dw_dt in ((ConvOpType.kForward, tv.bfloat16), (ConvOpType.kBackwardInput, tv.bfloat16),
+                          (ConvOpType.kBackwardWeight, tv.float32)):
+            p = ConvParams(3, op)
+            p.conv_algo_desp = find_desp(op, "Tcgen05", tv.bfloat16, dw_dt, tv.bfloat16, 128)
+            if op == ConvOpType.kForward:
+                o = torch.zeros((n, K), dtype=torch.bfloat16, device="cuda")
+                p.input, p.weight, p.output = tv.Tensor(x), tv.Tensor(w), tv.Tensor(o)
+                p.indices = tv.Tensor(pt.pairs_fwd)
+                p.mask = tv.Tensor(pt.masks_fwd[0], tv.uint32)
+                if use_sorted:
+                    p.indices_sorted = tv.Tensor(pt.sorted_indices("fwd"))
+            elif op == ConvOpType.kBackwardInput:
+                o = torch.zeros((n, C), dtype=torch.bfloat16, device="cuda")
+                p.input, p.weight, p.output = tv.Tensor(o), tv.Tensor(w), tv.Tensor(dy)
+                p.indices = tv.Tensor(pt.pairs_bwd)
+                p.mask = tv.Tensor(pt.masks_fwd[0], tv.uint32)
+                p.reverse_mask = True
+                if use_sorted:
+                    p.indices_sorted = tv.Tensor(pt.sorted_indices("bwd"))
+            else:
+                o = torch.zeros((K, 27, C), dtype=torch.float32, device="cuda")
+                mo = co.tile_masks(m, 128).astype(np.uint32)
+                p.input, p.weight, p.output = tv.Tensor(x), tv.Tensor(o), tv.Tensor(dy)
+                p.indices = tv.Tensor(pt.pairs_fwd)
+                p.mask = u32(mo)
+                p.mask_width = 128
+                if use_sorted:
+                    p.indices_sorted = tv.Tensor(pt.sorted_indices("fwd"))
+            p.mask_argsort = tv.Tensor(pt.argsorts_fwd[0])
+            ConvMainUnitTest(sync_check=True).implicit_gemm2(p)
+            res.append(o.float().cpu())
+        outs.append(res)
+    assert torch.equal(outs[0][0], outs[1][0])
+    assert torch.equal(outs[0][1], outs[1][1])
+    # wgrad accumulates per-CTA partial sums with fp32 atomics: equal up to the
+    # (run-to-run) summation order
+    nr = (torch.linalg.norm(outs[0][2] - outs[1][2]) / torch.linalg.norm(outs[0][2])).item()
+    assert nr < 1e-6, nr
