@@ -239,10 +239,23 @@ __global__ void __maxnreg__(96)
       const int n_tile = static_cast<int>(tile % A.n_tiles);
       const int64_t row_g = tile_m * kTileM + r;
       const bool valid = row_g < A.M;
-      int sig = valid ? (A.argsort ? __ldg(A.argsort + row_g) : static_cast<int>(row_g)) : -1;
-      if (valid && (sig < 0 || sig >= A.out_rows)) {
-        flag_error(A.err, kErrBadIndex);
-        sig = -1;
+      // With the sorted table every index load of the row leaves at once,
+      // together with the mask loads below (one memory round trip per tile);
+      // the argsort indirection is not needed here.
+      int pre[32];
+      int sig;
+      if (A.idx_sorted) {
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+          pre[k] = (valid && k < A.kv) ? __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.M + row_g)
+                                       : -1;
+        sig = valid ? 0 : -1;
+      } else {
+        sig = valid ? (A.argsort ? __ldg(A.argsort + row_g) : static_cast<int>(row_g)) : -1;
+        if (valid && (sig < 0 || sig >= A.out_rows)) {
+          flag_error(A.err, kErrBadIndex);
+          sig = -1;
+        }
       }
       // every loader warp reduces all four 32-row groups itself (no cross-warp
       // barrier, so an aborted warp can never strand the others)
@@ -291,8 +304,8 @@ __global__ void __maxnreg__(96)
           const int k = kb + q;
           int v = -1;
           if (k < A.kv && ((tm >> k) & 1u) && sig >= 0 && ((sub >> k) & 1u)) {
-            if (A.idx_sorted)  // coalesced: row_g is the sorted row
-              v = __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.M + row_g);
+            if (A.idx_sorted)  // already loaded (coalesced, row_g is the sorted row)
+              v = pre[k];
             else if (A.indices)
               v = __ldg(A.indices + static_cast<int64_t>(k) * A.M + sig);
             else
