@@ -427,6 +427,64 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
   return SC_OK;
 }
 
+// ------------------------------------------------ backward weight, static scratch
+// The weight-gradient kernels accumulate into an fp32 [K, kv, C] buffer.  This
+// entry point takes that buffer from a file-scope device array instead of the
+// caller's workspace, so a caller with no device allocator still gets dW.
+}  // extern "C"
+
+namespace {
+constexpr int64_t kStaticScratchFloats = int64_t(1) << 21;  // 8 MiB of fp32
+static __device__ __align__(256) float g_wgrad_scratch[kStaticScratchFloats];
+float *g_scratch_ptr[kMaxDevices] = {nullptr};
+
+// Address of this device's copy of g_wgrad_scratch, looked up once per device
+// (with that device current) and cached.
+int scratch_address(float **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail(SC_RUNTIME, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  if (g_scratch_ptr[dev] == nullptr) {
+    void *ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_wgrad_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(wgrad scratch)");
+    g_scratch_ptr[dev] = static_cast<float *>(ptr);
+  }
+  *out = g_scratch_ptr[dev];
+  return SC_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int sc_conv_wgrad_static_scratch(const sc_conv_params *p) {
+  g_last_error.clear();
+  if (p == nullptr) return fail(SC_INVALID_ARG, "params is null");
+  if (p->op_type != SC_CONV_BACKWARD_WEIGHT)
+    return fail(SC_INVALID_ARG, "sc_conv_wgrad_static_scratch runs backward weight only (op_type %d)",
+                p->op_type);
+  if (p->workspace != nullptr || p->workspace_bytes != 0)
+    return fail(SC_INVALID_ARG, "sc_conv_wgrad_static_scratch takes no workspace (it uses its own scratch)");
+  ConvPlan plan;
+  int rc = plan_conv(p, &plan);
+  if (rc != SC_OK) return rc;
+  const int64_t floats = p->K * p->kv * p->C;
+  if (floats > kStaticScratchFloats)
+    return fail(SC_INVALID_ARG,
+                "K*kv*C = %lld exceeds the static wgrad scratch of %lld floats (8 MiB); "
+                "use sc_conv_implicit_gemm with a workspace",
+                (long long)floats, (long long)kStaticScratchFloats);
+  float *scratch = nullptr;
+  rc = scratch_address(&scratch);
+  if (rc != SC_OK) return rc;
+  sc_conv_params q = *p;
+  q.workspace = scratch;
+  q.workspace_bytes = kStaticScratchFloats * 4;
+  return sc_conv_implicit_gemm(&q);
+}
+
 // ------------------------------------------------------------------ GEMM
 static int plan_gemm(const sc_gemm_params *p, scb::GemmArgs *a) {
   if (p == nullptr) return fail(SC_INVALID_ARG, "params is null");

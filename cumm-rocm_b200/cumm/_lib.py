@@ -21,6 +21,7 @@ EXPORTS = (
     "sc_pairs_workspace_size", "sc_build_subm_pairs", "sc_build_conv_outputs",
     "sc_build_conv_pairs", "sc_sort_masks_split", "sc_sort_workspace_size",
     "sc_check_device_error", "sc_last_error", "sc_version", "sc_sort_indices",
+    "sc_conv_wgrad_static_scratch",
 )
 
 c_i32, c_i64, c_u32, c_f32, c_vp = (ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32,

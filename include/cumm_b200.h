@@ -179,6 +179,23 @@ int sc_conv_implicit_gemm(const sc_conv_params *p);
  * bytes of workspace sc_conv_implicit_gemm needs for these params. */
 int sc_conv_workspace_size(const sc_conv_params *p, int64_t *bytes);
 
+/*
+ * Backward weight without a caller workspace.  No counterpart in the
+ * reference: implicit_gemm2 allocates a missing workspace itself
+ * (cumm/conv/nvrtc_code.py:181-196), this library never allocates.
+ * Same params and results as sc_conv_implicit_gemm with op_type
+ * SC_CONV_BACKWARD_WEIGHT; workspace must be NULL / 0.  The fp32 [K, kv, C]
+ * accumulator lives in a static 8 MiB device array of this library, so
+ * K * kv * C must be <= 2097152 (else SC_INVALID_ARG).  Nothing has to start
+ * at zero: each call clears the part it uses on p->stream before the kernel.
+ * The first call on a device (with that device current) looks up the array's
+ * address; make that first call before any stream capture starts.  There is
+ * one array per device: calls that may run at the same time on one device
+ * (different streams or host threads) race on it and give wrong gradients;
+ * calls queued on one stream are safe.
+ */
+int sc_conv_wgrad_static_scratch(const sc_conv_params *p);
+
 /* Replaces GemmMainUnitTest.matmul2 (cumm/gemm/main.py:1176-1335). */
 int sc_gemm_matmul(const sc_gemm_params *p);
 
