@@ -21,7 +21,8 @@
 //   warps 0-3   epilogue: TMEM -> registers -> permuted row stores
 //   warps 4-11  producers: 16-byte cp.async gathers of the A rows that have a
 //               pair into SWIZZLE_128B shared-memory stages (one 128-byte
-//               reduction chunk per stage); rows without a pair are
+//               reduction chunk per stage, 16 rows per warp, all warps on
+//               every stage); rows without a pair are
 //               zero-filled copies (no memory request; a shared store would
 //               need a proxy fence that waits on the thread's copies in
 //               flight); the weight slab arrives by one 2-D TMA load.
@@ -167,7 +168,7 @@ constexpr int kProdWarps = 8;
 constexpr int kLoadWarp0 = 12;   // warps 12-15
 constexpr int kMmaWarp = 16;
 
-template <bool kF8, typename TOut, bool kTma>
+template <bool kF8, typename TOut, bool kTma, bool kGather>
 __global__ void __maxnreg__(96)
     conv_rowgather_kernel(const __grid_constant__ KParams P) {
   extern __shared__ uint8_t smem_raw[];
@@ -194,14 +195,15 @@ __global__ void __maxnreg__(96)
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < S; ++i) {
-      // the 32 lanes of the stage's producer warp arrive through
-      // cp.async.mbarrier.arrive.noinc; with TMA one more arrive.expect_tx
-      mbar_init(&full_bar[i], 32 + (kTma ? 1 : 0));
+      // gather: one arrive.expect_tx per producer warp; cp.async: the 32
+      // lanes of the stage's producer warp (cp.async.mbarrier.arrive.noinc)
+      // plus, with TMA, one arrive.expect_tx for the weight slab
+      mbar_init(&full_bar[i], kGather ? kProdWarps : 32 + (kTma ? 1 : 0));
       mbar_init(&empty_bar[i], 1);
     }
     for (int i = 0; i < kIdxStages; ++i) {
       mbar_init(&idx_full[i], 128);
-      mbar_init(&idx_empty[i], min(S, kProdWarps) + 1);
+      mbar_init(&idx_empty[i], (kGather ? kProdWarps : min(S, kProdWarps)) + 1);
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(&acc_full[i], 1);
@@ -239,23 +241,29 @@ __global__ void __maxnreg__(96)
       const int n_tile = static_cast<int>(tile % A.n_tiles);
       const int64_t row_g = tile_m * kTileM + r;
       const bool valid = row_g < A.M;
-      // With the sorted table every index load of the row leaves at once,
-      // together with the mask loads below (one memory round trip per tile);
-      // the argsort indirection is not needed here.
+      // Every index of the row (all kv offsets) is loaded up front and stored
+      // unconditionally below, so the loads leave together: one memory round
+      // trip per tile.  With the sorted table row_g is already the sorted row;
+      // otherwise sigma(row) comes first (argsort), then the kv loads.
       int pre[32];
-      int sig;
       if (A.idx_sorted) {
 #pragma unroll
         for (int k = 0; k < 32; ++k)
           pre[k] = (valid && k < A.kv) ? __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.M + row_g)
                                        : -1;
-        sig = valid ? 0 : -1;
       } else {
-        sig = valid ? (A.argsort ? __ldg(A.argsort + row_g) : static_cast<int>(row_g)) : -1;
+        int sig = valid ? (A.argsort ? __ldg(A.argsort + row_g) : static_cast<int>(row_g)) : -1;
         if (valid && (sig < 0 || sig >= A.out_rows)) {
           flag_error(A.err, kErrBadIndex);
           sig = -1;
         }
+        int ident = -1;
+        if (!A.indices && sig >= 0) ident = A.a_inds ? __ldg(A.a_inds + row_g) : static_cast<int>(row_g);
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+          pre[k] = (sig >= 0 && k < A.kv)
+                       ? (A.indices ? __ldg(A.indices + static_cast<int64_t>(k) * A.M + sig) : ident)
+                       : -1;
       }
       // every loader warp reduces all four 32-row groups itself (no cross-warp
       // barrier, so an aborted warp can never strand the others)
@@ -295,36 +303,18 @@ __global__ void __maxnreg__(96)
         tm = __brev(tm) >> (32 - A.kv);
         sub = __brev(sub) >> (32 - A.kv);
       }
-      // 16 offsets per batch keeps the loads in flight without a 32-entry array
+      // tab[k][r]: index of row r for offset k (-1 where the row's sub-tile
+      // mask lacks k).  Written for every offset, whatever the tile mask: a
+      // select, not a branch, so no load is deferred to its use.
 #pragma unroll
-      for (int kb = 0; kb < 32; kb += 16) {
-        int vals[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int k = kb + q;
-          int v = -1;
-          if (k < A.kv && ((tm >> k) & 1u) && sig >= 0 && ((sub >> k) & 1u)) {
-            if (A.idx_sorted)  // already loaded (coalesced, row_g is the sorted row)
-              v = pre[k];
-            else if (A.indices)
-              v = __ldg(A.indices + static_cast<int64_t>(k) * A.M + sig);
-            else
-              v = A.a_inds ? __ldg(A.a_inds + row_g) : static_cast<int>(row_g);
+      for (int k = 0; k < 32; ++k) {
+        if (k < A.kv) {
+          int v = ((sub >> k) & 1u) ? pre[k] : -1;
+          if (v < -1 || v >= A.a_rows) {
+            flag_error(A.err, kErrBadIndex);
+            v = -1;
           }
-          vals[q] = v;
-        }
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int k = kb + q;
-          if (k < A.kv && ((tm >> k) & 1u)) {
-            int v = vals[q];
-            if (v < -1 || v >= A.a_rows) {
-              flag_error(A.err, kErrBadIndex);
-              v = -1;
-            }
-            const int slot = __popc(tm & ((1u << k) - 1u));
-            tab[slot * kTileM + r] = v;
-          }
+          tab[k * kTileM + r] = v;
         }
       }
       if (r == 0) {
@@ -344,6 +334,74 @@ __global__ void __maxnreg__(96)
     }
   } else if (warp >= kProdWarp0 && warp < kProdWarp0 + kProdWarps) {
     // ---------------------------------------------------------------- producers
+    const int pw = warp - kProdWarp0;
+    if constexpr (kGather) {
+    // TMA gather: all kProdWarps warps serve every chunk; lanes 0-3 of warp pw
+    // each issue one tile::gather4 (4 rows x 128 bytes, SWIZZLE_128B by
+    // address) for rows [16 pw, 16 pw + 16) of the stage.  An index of -1 is
+    // an out-of-range row and lands as zeros.  Lane 0 of every warp arrives
+    // with expect_tx for its 2 KB (one warp in turn adds the weight slab), so
+    // a stage completes on kProdWarps arrivals plus the copied bytes.  Every
+    // warp arrives once per use of stage s and empty phase n cannot complete
+    // before all of them did, so no warp runs two phases ahead of a wait.
+    // (Measured on B200: 8 warps of gather4 fill a 16 KB stage in ~740
+    // cycles; per-thread cp.async arrivals serialise on the barrier word.)
+    const int esz = kF8 ? 1 : 2;
+    const int box = 128 / esz;
+    const uint32_t a_tx = (kTileM / kProdWarps) * 128u;
+    const uint32_t b_tx = static_cast<uint32_t>(A.BN) * 128;
+    const int r0 = pw * (kTileM / kProdWarps) + lane * 4;
+    int it = 0;
+    uint32_t stage = 0, eph = 0, gchunk = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < P.num_tiles && ok; tile += gridDim.x, ++it) {
+      const int b = it % kIdxStages;
+      const uint32_t ph = (it / kIdxStages) & 1;
+      if (!__all_sync(0xffffffffu, mbar_wait(&idx_full[b], ph, abort_flag))) {
+        if (lane == 0) flag_error(A.err, kErrWaitTimeout);
+        break;
+      }
+      const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
+      const int *tab = reinterpret_cast<const int *>(buf);
+      const Meta *meta = reinterpret_cast<const Meta *>(buf + A.kv * kTileM * 4);
+      const int nch = meta->nchunks;
+      const int n0 = (tile % A.n_tiles) * A.BN;
+      for (int j = 0; j < nch; ++j) {
+        const uint32_t s = stage;
+        const int slot_a = j / P.cpo;
+        const int cb = j - slot_a * P.cpo;
+        const int k = meta->k_list[slot_a];
+        const uint32_t sA = smem_base + s * P.stage_bytes;
+        if (!__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], eph ^ 1, abort_flag))) {
+          if (lane == 0) flag_error(A.err, kErrWaitTimeout);
+          ok = false;
+          break;
+        }
+        if (lane == 0) {
+          if (static_cast<int>(gchunk % kProdWarps) == pw) {
+            mbar_arrive_expect_tx(&full_bar[s], a_tx + b_tx);
+            tma_load_2d(sA + P.b_off, &P.tmap_b, k * (A.b_off_stride / esz) + cb * box, n0,
+                        &full_bar[s]);
+          } else {
+            mbar_arrive_expect_tx(&full_bar[s], a_tx);
+          }
+        }
+        __syncwarp();
+        if (lane < (kTileM / kProdWarps) / 4) {
+          const int4 q = *reinterpret_cast<const int4 *>(tab + k * kTileM + r0);
+          tma_gather4(sA + r0 * 128, &P.tmap_a, cb * box, q.x, q.y, q.z, q.w, &full_bar[s]);
+        }
+        ++gchunk;
+        if (++stage == static_cast<uint32_t>(S)) {
+          stage = 0;
+          eph ^= 1u;
+        }
+      }
+      if (!ok) break;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&idx_empty[b]);
+    }
+    } else {
     // Producer warp pw owns shared-memory stage pw (S <= kProdWarps stages;
     // warps beyond S stay idle) and fills every chunk c with c % S == pw
     // alone: lane owns 16-byte unit u of rows rg + 4 i (i < 32).  The S stages
@@ -354,7 +412,6 @@ __global__ void __maxnreg__(96)
     // Rows with a pair are fetched with 16-byte cp.async; rows without one are
     // zero-filled cp.async (src-size 0, no memory request).  With TMA the
     // weight slab is one 2-D tiled load issued by lane 0.
-    const int pw = warp - kProdWarp0;
     const int u = lane & 7;
     const int rg = lane >> 3;
     const int esz = kF8 ? 1 : 2;
@@ -421,7 +478,7 @@ __global__ void __maxnreg__(96)
           byte0 = (u % P.upo) * 16;
         }
         const bool slot_ok = slot < na && byte0 < A.a_row_bytes;
-        const int *trow = tab + slot * kTileM;
+        const int *trow = tab + (slot_ok ? meta->k_list[slot] : 0) * kTileM;
         const uint8_t *abase = A.a_base + byte0;
 #pragma unroll 8
         for (int i = 0; i < kTileM / 4; ++i) {
@@ -468,6 +525,7 @@ __global__ void __maxnreg__(96)
       if (lane == 0) mbar_arrive(&idx_empty[b]);
     }
     cp_async_wait_all();
+    }
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
@@ -592,9 +650,11 @@ __global__ void __maxnreg__(96)
 }
 
 template <bool kF8, typename TOut>
-cudaError_t launch_typed(const KParams &P, bool tma, int grid, size_t smem, cudaStream_t stream) {
-  void (*kern)(KParams) =
-      tma ? conv_rowgather_kernel<kF8, TOut, true> : conv_rowgather_kernel<kF8, TOut, false>;
+cudaError_t launch_typed(const KParams &P, bool tma, bool gather, int grid, size_t smem,
+                         cudaStream_t stream) {
+  void (*kern)(KParams) = gather ? conv_rowgather_kernel<kF8, TOut, true, true>
+                          : tma  ? conv_rowgather_kernel<kF8, TOut, true, false>
+                                 : conv_rowgather_kernel<kF8, TOut, false, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
@@ -639,27 +699,31 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
   if (P.num_tiles == 0) return cudaSuccess;
   const int grid = static_cast<int>(P.num_tiles < num_sms ? P.num_tiles : num_sms);
   // TMA weight slabs: whole 128-byte reduction chunks (no packing of small offsets)
-  bool tma = false;
+  bool tma = false, gather = false;
   if (P.cpo > 0) {
     const int esz = a.in_dtype == 14 ? 1 : 2;
     const uint32_t box = 128u / esz;
     const uint64_t red = static_cast<uint64_t>(a.a_row_bytes) / esz;
     tma = encode_tmap_2d(&P.tmap_b, a.in_dtype, a.b_base, red * a.kv, a.n_total,
                          static_cast<uint64_t>(a.b_row_stride), box, a.BN);
+    // gathered A rows: [a_rows, red] with one-row boxes (tile::gather4)
+    if (tma && a.a_row_bytes >= 128 && a.a_rows > 0)
+      gather = encode_tmap_2d(&P.tmap_a, a.in_dtype, a.a_base, red, static_cast<uint64_t>(a.a_rows),
+                              static_cast<uint64_t>(a.a_row_stride), box, 1);
   }
   if (a.in_dtype == 14) {
     P.idesc = make_idesc(128, a.BN, 0u, false, false);
     switch (a.out_dtype) {
-      case 0: return launch_typed<true, float>(P, tma, grid, smem, stream);
-      case 7: return launch_typed<true, __half>(P, tma, grid, smem, stream);
-      default: return launch_typed<true, __nv_bfloat16>(P, tma, grid, smem, stream);
+      case 0: return launch_typed<true, float>(P, tma, gather, grid, smem, stream);
+      case 7: return launch_typed<true, __half>(P, tma, gather, grid, smem, stream);
+      default: return launch_typed<true, __nv_bfloat16>(P, tma, gather, grid, smem, stream);
     }
   }
   P.idesc = make_idesc(128, a.BN, a.in_dtype == 12 ? 1u : 0u, false, false);
   switch (a.out_dtype) {
-    case 0: return launch_typed<false, float>(P, tma, grid, smem, stream);
-    case 7: return launch_typed<false, __half>(P, tma, grid, smem, stream);
-    case 12: return launch_typed<false, __nv_bfloat16>(P, tma, grid, smem, stream);
+    case 0: return launch_typed<false, float>(P, tma, gather, grid, smem, stream);
+    case 7: return launch_typed<false, __half>(P, tma, gather, grid, smem, stream);
+    case 12: return launch_typed<false, __nv_bfloat16>(P, tma, gather, grid, smem, stream);
     default: break;
   }
   return cudaErrorInvalidValue;
