@@ -13,8 +13,8 @@
 // staged MN-major: a 64-row chunk of gathered input rows (two 128-byte atoms =
 // 128 MN-elements: one or more filters' channels) is the M side and the
 // matching 64 dOut rows are the N side.  Every CTA owns a group of M-tiles
-// (up to 512 TMEM columns of fp32 accumulators) and a contiguous range of row
-// chunks; TMEM accumulates over the whole range, and the epilogue adds the
+// (up to 512 TMEM columns of fp32 accumulators) and every splits-th row
+// chunk; TMEM accumulates over the whole range, and the epilogue adds the
 // CTA's partial dW into an fp32 workspace with red.global.add (split over rows
 // without a serial semaphore, so there is no inter-CTA spin).  A finalize
 // kernel applies alpha/beta and converts to the weight dtype.
@@ -133,8 +133,11 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
   const int g = blockIdx.y;
   int k_lo, k_hi, t0, t1;
   group_filters(P, g, k_lo, k_hi, t0, t1);
-  const int c_begin = blockIdx.x * P.chunks_per_cta;
-  const int c_end = min(c_begin + P.chunks_per_cta, P.n_chunks);
+  // chunks are dealt round-robin (c = x, x + splits, ...): rows are sorted by
+  // mask, so contiguous ranges would give some CTAs only the dense chunks
+  const int c_begin = blockIdx.x;
+  const int c_end = P.n_chunks;
+  const int c_step = gridDim.x;
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < S; ++i) {
@@ -166,7 +169,7 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
     const int r = t & 63;       // row of the chunk
     const int half = t >> 6;    // filter parity handled by this thread
     int it = 0;
-    for (int c = c_begin; c < c_end; ++c, ++it) {
+    for (int c = c_begin; c < c_end; c += c_step, ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
       if (!mbar_wait(&idx_empty[b], ph ^ 1, abort_flag)) {
@@ -216,18 +219,21 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       for (int s = 16; s > 0; s >>= 1) gw |= __shfl_xor_sync(0xffffffffu, gw, s);
       if (half == 0) sig_tab[r] = sig;
       const uint32_t cm = gw;
+      // every index of the thread's filters is loaded up front and gated by a
+      // select afterwards, so the loads leave together (one round trip)
       int vals[16];
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
         const int k = k_lo + 2 * q + half;
         int v = -1;
-        if (k < k_hi && ((word >> k) & 1u) && sig >= 0) {
-          if (A.idx_sorted)  // coalesced: row is the sorted row
-            v = __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.N + row);
-          else if (A.indices)
-            v = __ldg(A.indices + static_cast<int64_t>(k) * A.N + sig);
-          else
+        if (k < k_hi) {
+          if (A.idx_sorted) {  // coalesced: row is the sorted row
+            if (valid) v = __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.N + row);
+          } else if (A.indices) {
+            if (sig >= 0) v = __ldg(A.indices + static_cast<int64_t>(k) * A.N + sig);
+          } else if (sig >= 0) {
             v = A.b_inds ? __ldg(A.b_inds + row) : static_cast<int>(row);
+          }
         }
         vals[q] = v;
       }
@@ -235,7 +241,7 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       for (int q = 0; q < 16; ++q) {
         const int k = k_lo + 2 * q + half;
         if (k < k_hi) {
-          int v = vals[q];
+          int v = (((word >> k) & 1u) && sig >= 0) ? vals[q] : -1;
           if (v < -1 || v >= A.in_rows) {
             flag_error(A.err, kErrBadIndex);
             v = -1;
@@ -271,7 +277,7 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
     bool ok = pw < S;
     const uint32_t uS = static_cast<uint32_t>(S);
     const int n_b_atoms = P.n_mma / 64;
-    for (int c = c_begin; c < c_end && ok; ++c, ++it) {
+    for (int c = c_begin; c < c_end && ok; c += c_step, ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
       int w_ok = 1;
@@ -361,7 +367,7 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       uint32_t stage = 0, fph = 0;
       uint32_t started = 0;
       bool ok = true;
-      for (int c = c_begin; c < c_end && ok; ++c, ++it) {
+      for (int c = c_begin; c < c_end && ok; c += c_step, ++it) {
         const int b = it % kIdxStages;
         const uint32_t ph = (it / kIdxStages) & 1;
         if (!mbar_wait(&idx_full[b], ph, abort_flag)) {
@@ -508,6 +514,9 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t 
   int per_group = 512 / P.n_mma;
   if (per_group > 16) per_group = 16;
   if (per_group > P.n_mtiles) per_group = P.n_mtiles;
+  // as few groups as TMEM allows, then equal shares (14 tiles: 7 + 7, not 8 + 6)
+  const int n_groups = (P.n_mtiles + per_group - 1) / per_group;
+  per_group = (P.n_mtiles + n_groups - 1) / n_groups;
   P.tiles_per_group = per_group;
   P.n_groups = (P.n_mtiles + per_group - 1) / per_group;
   int splits = (num_sms + P.n_groups - 1) / P.n_groups;
