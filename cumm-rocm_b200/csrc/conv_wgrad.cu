@@ -20,6 +20,8 @@
 // kernel applies alpha/beta and converts to the weight dtype.
 // Warp roles are the same as the forward kernel: 0-3 epilogue, 4-11 cp.async
 // producers, 12-15 index loaders, 16 TMEM allocator + tcgen05.mma issuer.
+#include <cuda.h>
+
 #include "kernels.h"
 
 namespace scb {
@@ -41,6 +43,8 @@ struct WMeta {
 };
 
 struct WParams {
+  CUtensorMap tmap_in;    // input rows [in_rows, C], one-row boxes (gather path)
+  CUtensorMap tmap_dout;  // dOut rows [dout_rows, K], one-row boxes (gather path)
   ConvWgradArgs a;
   int n_chunks;        // ceil(N / 64)
   int chunks_per_cta;
@@ -55,6 +59,7 @@ struct WParams {
   int stages;
   uint32_t stage_bytes;
   uint32_t b_off;
+  uint32_t bbuf_off;      // gather path: two dOut buffers of n_b_atoms x 8 KB
   uint32_t idx_off;
   uint32_t idx_buf_bytes;
   uint32_t bar_off;
@@ -107,7 +112,7 @@ __device__ __forceinline__ uint32_t tile_filter_bits(const WParams &P, int t) {
   return upto_hi & ~((1u << lo) - 1u);
 }
 
-template <int kLag>
+template <bool kGather>
 __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParams P) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_u32 = smem_u32(smem_raw);
@@ -124,7 +129,9 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
   uint64_t *idx_empty = idx_full + kIdxStages;
   uint64_t *acc_full = idx_empty + kIdxStages;
   uint64_t *drain_bar = acc_full + 1;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain_bar + 1);
+  uint64_t *bfull = drain_bar + 1;   // gather path: dOut buffer b loaded
+  uint64_t *bempty = bfull + 2;      // gather path: dOut buffer b consumed
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bempty + 2);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
   uint32_t *used_tiles = reinterpret_cast<uint32_t *>(tmem_slot + 2);
 
@@ -141,15 +148,21 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < S; ++i) {
-      mbar_init(&full_bar[i], 32);
+      // gather: one arrive.expect_tx per producer warp; cp.async: the 32
+      // lanes of the stage's producer warp (cp.async.mbarrier.arrive.noinc)
+      mbar_init(&full_bar[i], kGather ? kProdWarps : 32);
       mbar_init(&empty_bar[i], 1);
     }
     for (int i = 0; i < kIdxStages; ++i) {
       mbar_init(&idx_full[i], 128);
-      mbar_init(&idx_empty[i], min(S, kProdWarps) + 1);
+      mbar_init(&idx_empty[i], (kGather ? kProdWarps : min(S, kProdWarps)) + 1);
     }
     mbar_init(acc_full, 1);
     mbar_init(drain_bar, 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&bfull[i], kProdWarps);
+      mbar_init(&bempty[i], 1);
+    }
     *abort_flag = 0;
     *used_tiles = 0;
     fence_mbar_init();
@@ -270,6 +283,78 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
     // Gathered rows with a pair use cp.async, the others are zero-filled
     // cp.async (src-size 0, no memory request).
     const int pw = warp - kProdWarp0;
+    if constexpr (kGather) {
+    // TMA gather: all kProdWarps warps serve every stage.  Lane l < 4 of warp
+    // pw issues one tile::gather4 for rows 8 pw + 4 (l & 1) .. +3 of atom
+    // l >> 1 (input rows of the atom's filter; index -1 lands as zeros).
+    // The chunk's 64 dOut rows are the same for every M-tile, so they are
+    // gathered once per chunk into one of two dOut buffers (lanes
+    // l < 2 n_b_atoms, same row split), released by the MMA after the chunk's
+    // last tile.  Lane 0 of each warp arrives with expect_tx for its bytes.
+    const int n_b_atoms = P.n_mma / 64;
+    const int rq = pw * 8 + (lane & 1) * 4;
+    int it = 0;
+    uint32_t stage = 0, eph = 0, ub = 0;
+    bool ok = true;
+    for (int c = c_begin; c < c_end && ok; c += c_step, ++it) {
+      const int b = it % kIdxStages;
+      const uint32_t ph = (it / kIdxStages) & 1;
+      if (!__all_sync(0xffffffffu, mbar_wait(&idx_full[b], ph, abort_flag))) {
+        if (lane == 0) flag_error(A.err, kErrWaitTimeout);
+        break;
+      }
+      const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
+      const int *tab = reinterpret_cast<const int *>(buf);
+      const int *sig_tab = tab + 32 * kRows;
+      const WMeta *meta = reinterpret_cast<const WMeta *>(sig_tab + kRows);
+      uint32_t bits = meta->active_bits;
+      if (bits) {
+        const uint32_t bb = ub & 1u;
+        if (!__all_sync(0xffffffffu, mbar_wait(&bempty[bb], ((ub >> 1) & 1u) ^ 1u, abort_flag))) {
+          if (lane == 0) flag_error(A.err, kErrWaitTimeout);
+          break;
+        }
+        if (lane == 0) mbar_arrive_expect_tx(&bfull[bb], static_cast<uint32_t>(n_b_atoms) * 1024u);
+        __syncwarp();
+        if (lane < 2 * n_b_atoms) {
+          const int na = lane >> 1;
+          const int4 q = *reinterpret_cast<const int4 *>(sig_tab + rq);
+          tma_gather4(smem_base + P.bbuf_off + bb * (n_b_atoms * 8192u) + na * 8192u + rq * 128,
+                      &P.tmap_dout, na * 64, q.x, q.y, q.z, q.w, &bfull[bb]);
+        }
+        ++ub;
+      }
+      while (bits) {
+        const int jt = __ffs(bits) - 1;
+        bits &= bits - 1;
+        const int tt = t0 + jt;
+        const uint32_t s = stage;
+        if (!__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], eph ^ 1, abort_flag))) {
+          if (lane == 0) flag_error(A.err, kErrWaitTimeout);
+          ok = false;
+          break;
+        }
+        if (++stage == static_cast<uint32_t>(S)) {
+          stage = 0;
+          eph ^= 1u;
+        }
+        if (lane == 0) mbar_arrive_expect_tx(&full_bar[s], 2048u);
+        __syncwarp();
+        if (lane < 4) {
+          const int a = 2 * tt + (lane >> 1);
+          const int k = a / P.cpa;
+          int4 q = make_int4(-1, -1, -1, -1);
+          if (a < P.n_atoms && k < A.kv)
+            q = *reinterpret_cast<const int4 *>(tab + (k - k_lo) * kRows + rq);
+          tma_gather4(smem_base + s * P.stage_bytes + (lane >> 1) * 8192u + rq * 128, &P.tmap_in,
+                      (a % P.cpa) * 64, q.x, q.y, q.z, q.w, &full_bar[s]);
+        }
+      }
+      if (!ok) break;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&idx_empty[b]);
+    }
+    } else {
     const int u = lane & 7;
     const int rg = lane >> 3;
     int it = 0;
@@ -360,11 +445,12 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       if (lane == 0) mbar_arrive(&idx_empty[b]);
     }
     cp_async_wait_all();
+    }
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
       int it = 0;
-      uint32_t stage = 0, fph = 0;
+      uint32_t stage = 0, fph = 0, ub = 0;
       uint32_t started = 0;
       bool ok = true;
       for (int c = c_begin; c < c_end && ok; c += c_step, ++it) {
@@ -378,6 +464,15 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
                                                             (32 * kRows + kRows) * 4);
         uint32_t bits = meta->active_bits;
         mbar_arrive(&idx_empty[b]);
+        uint32_t sBg = 0;
+        const bool chunk_used = bits != 0;
+        if (kGather && chunk_used) {
+          if (!mbar_wait(&bfull[ub & 1u], (ub >> 1) & 1u, abort_flag)) {
+            flag_error(A.err, kErrWaitTimeout);
+            break;
+          }
+          sBg = smem_base + P.bbuf_off + (ub & 1u) * ((P.n_mma / 64) * 8192u);
+        }
         while (bits) {
           const int j = __ffs(bits) - 1;
           bits &= bits - 1;
@@ -389,7 +484,7 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
           }
           tc_fence_after();
           const uint32_t sA = smem_base + s * P.stage_bytes;
-          const uint32_t sB = sA + P.b_off;
+          const uint32_t sB = kGather ? sBg : sA + P.b_off;
           const uint32_t d = tmem_base + static_cast<uint32_t>(j * P.n_mma);
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk) {
@@ -404,6 +499,10 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
             stage = 0;
             fph ^= 1u;
           }
+        }
+        if (kGather && chunk_used && ok) {
+          mma_commit(&bempty[ub & 1u]);  // dOut buffer free once these MMAs finish
+          ++ub;
         }
       }
       if (started) {
@@ -523,35 +622,37 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t 
   if (splits > P.n_chunks) splits = P.n_chunks;
   P.chunks_per_cta = (P.n_chunks + splits - 1) / splits;
   splits = (P.n_chunks + P.chunks_per_cta - 1) / P.chunks_per_cta;
+  // gather path: whole 128-byte row blocks on both sides and tensor maps for
+  // the input and dOut rows (else 16-byte cp.async gathers)
+  bool gather = P.cpa > 0 && a.K % 64 == 0 && (a.in_dtype == 12 || a.in_dtype == 7) &&
+                a.in_rows > 0 && a.dout_rows > 0;
+  if (gather)
+    gather = encode_tmap_2d(&P.tmap_in, a.in_dtype, a.input, static_cast<uint64_t>(a.C),
+                            static_cast<uint64_t>(a.in_rows), static_cast<uint64_t>(a.in_ld) * 2, 64, 1) &&
+             encode_tmap_2d(&P.tmap_dout, a.in_dtype, a.dout, static_cast<uint64_t>(a.K),
+                            static_cast<uint64_t>(a.dout_rows), static_cast<uint64_t>(a.dout_ld) * 2, 64, 1);
   const uint32_t a_bytes = 2 * 8192;
   const uint32_t b_bytes = static_cast<uint32_t>(P.n_mma / 64) * 8192;
-  P.stage_bytes = a_bytes + b_bytes;
+  P.stage_bytes = gather ? a_bytes : a_bytes + b_bytes;
   P.b_off = a_bytes;
+  const uint32_t bbuf_bytes = gather ? 2 * b_bytes : 0;
   P.idx_buf_bytes = ((32 * kRows + kRows) * 4 + sizeof(WMeta) + 127) & ~127u;
   const uint32_t idx_total = P.idx_buf_bytes * kIdxStages;
   const uint32_t bar_bytes = 512;
-  const uint32_t budget = 227u * 1024u - 1024u - idx_total - bar_bytes;
+  const uint32_t budget = 227u * 1024u - 1024u - idx_total - bar_bytes - bbuf_bytes;
   int stages = static_cast<int>(budget / P.stage_bytes);
   if (stages > 8) stages = 8;
   if (stages < 2) return cudaErrorInvalidConfiguration;
   P.stages = stages;
-  P.idx_off = P.stage_bytes * stages;
+  P.bbuf_off = P.stage_bytes * stages;
+  P.idx_off = P.bbuf_off + bbuf_bytes;
   P.bar_off = P.idx_off + idx_total;
   const size_t smem = 1024 + P.bar_off + bar_bytes;
   uint32_t cols = 32;
   while (cols < static_cast<uint32_t>(per_group * P.n_mma)) cols <<= 1;
   P.tmem_cols = cols;
   P.idesc = make_idesc(128, P.n_mma, a.in_dtype == 12 ? 1u : 0u, true, true);
-  int lag = stages - 2;
-  if (lag > 4) lag = 4;
-  if (lag < 1) lag = 1;
-  void (*kern)(WParams) = nullptr;
-  switch (lag) {
-    case 1: kern = conv_wgrad_kernel<1>; break;
-    case 2: kern = conv_wgrad_kernel<2>; break;
-    case 3: kern = conv_wgrad_kernel<3>; break;
-    default: kern = conv_wgrad_kernel<4>; break;
-  }
+  void (*kern)(WParams) = gather ? conv_wgrad_kernel<true> : conv_wgrad_kernel<false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
