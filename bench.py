@@ -349,9 +349,16 @@ def run_b200(args, rank, world, dist):
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
         traffic = json.loads(tfile.read_text()).get(names[dom])
+    # algorithmic bytes of one op: features in + out (or dOut + In for wgrad),
+    # weights, the [kv, N] index table, masks and argsort
+    alg_bytes = (N_VOX * C * 2 + N_VOX * K * 2 + KV * C * K * (4 if dom == 2 else 2)
+                 + KV * N_VOX * 4 + 2 * N_VOX * 4)
+    hbm_achieved = alg_bytes / (ms_op[dom] * 1e-3) / 1e9
     roofline = {"bound": "tensor", "kernel": names[dom], "achieved": achieved, "peak": peak_tf,
                 "unit": "TFLOP/s", "frac": achieved / peak_tf, "peak_kind": peak_kind,
-                "traffic": traffic}
+                "traffic": traffic,
+                "hbm": {"algorithmic_bytes": alg_bytes, "achieved_gbs": hbm_achieved,
+                        "peak_gbs": peak_bw, "frac": hbm_achieved / peak_bw}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -378,8 +385,9 @@ def run_b200(args, rank, world, dist):
             "per_op_tflops": {names[i]: flops_op / (ms_op[i] * 1e-3) / 1e12 for i in range(3)},
             "pct_bf16_peak": value / world / peak_tf,
             "roofline": roofline,
-            "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+            "e2e": None if n_e2e == 0 else {
+                "value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
             "cpu_baseline": cpu,
             "gpu_launches": 5 * args.steps,
             "clocks": clocks,
