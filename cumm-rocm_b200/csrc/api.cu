@@ -164,6 +164,12 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
     return SC_OK;
   }
   if (p->algo != SC_ALGO_TCGEN05) return fail(SC_RUNTIME, "Can't Found Algorithm: unknown algo %d", p->algo);
+  if (p->tile_n != 0 && op != SC_CONV_BACKWARD_WEIGHT) {
+    const int64_t ncols = op == SC_CONV_FORWARD ? p->K : p->C;
+    if (p->tile_n < 16 || p->tile_n > 256 || p->tile_n % 16 || ncols % p->tile_n)
+      return fail(SC_INVALID_ARG, "tile_n %d must be a multiple of 16, <= 256, dividing %lld",
+                  p->tile_n, (long long)ncols);
+  }
   if (op == SC_CONV_FORWARD) {
     const bool f8 = di == SC_FLOAT_E4M3 && dw == SC_FLOAT_E4M3;
     const bool f16 = is16(di) && dw == di;
@@ -356,10 +362,15 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     a.n_total = static_cast<int>(ncols);
     int tiles = 1;
     int64_t bn = ncols;
-    while (bn > 256 || bn % 16) {
-      ++tiles;
-      while (ncols % tiles || (ncols / tiles) % 16) ++tiles;
-      bn = ncols / tiles;
+    if (p->tile_n > 0) {
+      bn = p->tile_n;
+      tiles = static_cast<int>(ncols / bn);
+    } else {
+      while (bn > 256 || bn % 16) {
+        ++tiles;
+        while (ncols % tiles || (ncols / tiles) % 16) ++tiles;
+        bn = ncols / tiles;
+      }
     }
     a.BN = static_cast<int>(bn);
     a.n_tiles = tiles;

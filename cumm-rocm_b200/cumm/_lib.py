@@ -40,7 +40,7 @@ class ConvParamsC(ctypes.Structure):
         ("act_alpha", c_f32), ("act_beta", c_f32), ("act_type", c_i32), ("bias", c_vp),
         ("output_add", c_vp), ("scale", c_vp), ("split_k_slices", c_i32), ("flags", c_i32),
         ("workspace", c_vp), ("workspace_bytes", c_i64), ("stream", c_vp),
-        ("indices_sorted", c_vp),
+        ("indices_sorted", c_vp), ("tile_n", c_i32),
     ]
 
 

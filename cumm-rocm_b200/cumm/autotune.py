@@ -1,0 +1,104 @@
+"""Autotuner for the mask-implicit-GEMM forward: picks the mask split
+(MaskImplicitGemm = 1 launch, MaskSplitImplicitGemm = 2 launches over the two
+halves of the kernel offsets, spconv's ConvAlgo choice) and the output-column
+tile (ConvAlgoDesp tile_shape[1], ConvParams.tile_n) by timing each candidate
+on the caller's own workload with CUDA events, and caches the winner per
+workload signature (rows rounded up to a power of two, C, K, dtype).
+
+The reference picks its kernel from a fixed if-tree over tile shapes
+(cumm/conv/main.py:483-745, 'Can't Found Algorithm' when none fits); here the
+candidates all compute the same result and only their speed differs.
+"""
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Sequence, Tuple
+
+import torch
+
+from cumm import tensorview as tv
+from cumm.conv.main import ConvMainUnitTest, get_all_conv_algo_desp
+from cumm.tensorview.gemm import ConvOpType, ConvParams
+
+
+@dataclass(frozen=True)
+class FwdConfig:
+    num_split: int = 1   # 1: one launch with the full mask; 2: two launches, beta = 1 on the second
+    tile_n: int = 0      # 0: widest column tile
+
+    def __str__(self):
+        return f"split{self.num_split}_tn{self.tile_n or 'auto'}"
+
+
+def fwd_candidates(K: int) -> List[FwdConfig]:
+    res = [FwdConfig(1, 0), FwdConfig(2, 0)]
+    if K % 32 == 0 and K // 2 >= 16:
+        res.append(FwdConfig(1, K // 2))
+    return res
+
+
+def _desp(dt_in, dt_out):
+    for d in get_all_conv_algo_desp():
+        if (d.op_type == ConvOpType.kForward and d.algo == "Tcgen05" and d.dtype_input == dt_in
+                and d.dtype_weight == dt_in and d.dtype_output == dt_out and d.tile_shape[0] == 128):
+            return d
+    raise KeyError((dt_in, dt_out))
+
+
+def run_forward(cfg: FwdConfig, x: torch.Tensor, w: torch.Tensor, out: torch.Tensor, tables: Dict,
+                dt_in=tv.bfloat16, dt_out=tv.bfloat16, stream: int = 0, cm: ConvMainUnitTest = None):
+    """Forward conv of one (possibly batched) cloud with configuration `cfg`.
+    `tables[num_split]` is the PairTable built with that split count."""
+    pt = tables[cfg.num_split]
+    cm = cm or ConvMainUnitTest()
+    desp = _desp(dt_in, dt_out)
+    for j in range(cfg.num_split):
+        p = ConvParams(3, ConvOpType.kForward)
+        p.conv_algo_desp = desp
+        p.input, p.weight, p.output = tv.Tensor(x, dt_in), tv.Tensor(w, dt_in), tv.Tensor(out, dt_out)
+        p.indices = tv.Tensor(pt.pairs_fwd)
+        p.mask = tv.Tensor(pt.masks_fwd[j], tv.uint32)
+        p.mask_argsort = tv.Tensor(pt.argsorts_fwd[j])
+        p.indices_sorted = tv.Tensor(pt.sorted_indices("fwd", j))
+        p.mask_filter = pt.split_masks[j] if cfg.num_split > 1 else 0xffffffff
+        p.beta = 1.0 if j > 0 else 0.0
+        p.tile_n = cfg.tile_n
+        p.stream = stream or torch.cuda.current_stream().cuda_stream
+        cm.implicit_gemm2(p)
+
+
+@dataclass
+class ConvAutotuner:
+    iters: int = 5
+    cache: Dict[Tuple, FwdConfig] = field(default_factory=dict)
+    last_timings: Dict[str, float] = field(default_factory=dict)
+
+    @staticmethod
+    def key(n_rows: int, C: int, K: int, dt) -> Tuple:
+        b = 1
+        while b < n_rows:
+            b <<= 1
+        return ("fwd", b, C, K, int(dt))
+
+    def tune_forward(self, n_rows: int, C: int, K: int, dt, run: Callable[[FwdConfig], None],
+                     candidates: Sequence[FwdConfig] = None) -> FwdConfig:
+        """run(cfg) must launch one forward of the workload with `cfg` on the
+        current stream.  Returns (and caches) the fastest candidate."""
+        k = self.key(n_rows, C, K, dt)
+        if k in self.cache:
+            return self.cache[k]
+        cands = list(candidates or fwd_candidates(K))
+        times = {}
+        for cfg in cands:
+            run(cfg)  # warm-up (first-call set-up, L2)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(self.iters):
+                run(cfg)
+            e1.record()
+            torch.cuda.synchronize()
+            times[str(cfg)] = e0.elapsed_time(e1) / self.iters
+        best = min(cands, key=lambda c: times[str(c)])
+        self.cache[k] = best
+        self.last_timings = times
+        return best

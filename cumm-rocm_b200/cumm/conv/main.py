@@ -145,6 +145,7 @@ def build_conv_params_c(params: ConvParams) -> Tuple[_lib.ConvParamsC, dict]:
             raise ValueError("indices_sorted must have the shape of indices")
         _check_dense(isorted, "indices_sorted")
         cp.indices_sorted = isorted.byte_pointer()
+    cp.tile_n = int(getattr(params, "tile_n", 0) or 0)
     return cp, {"kv": kv, "C": C, "K": K}
 
 

@@ -408,3 +408,6 @@ class ConvParams:
         # mask_argsort order (SpconvOps.sort_indices); lets the kernels read
         # the index table coalesced; results are identical
         self.indices_sorted = Tensor()
+        # extension: output-column tile of the tcgen05 fwd / dgrad kernels
+        # (0 = widest); set by cumm.autotune, results are identical
+        self.tile_n = 0

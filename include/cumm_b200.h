@@ -123,6 +123,11 @@ typedef struct sc_conv_params {
    * coalesced instead of through the argsort indirection; results are
    * identical. */
   const int32_t *indices_sorted;
+  /* Output-column tile of the tcgen05 forward / backward-input kernels (the
+   * reference's ConvAlgoDesp tile_shape[1]): 0 picks the widest tile (all
+   * columns up to 256); otherwise a multiple of 16, <= 256, dividing the
+   * output width (K forward, C backward-input), else SC_INVALID_ARG. */
+  int32_t tile_n;
 } sc_conv_params;
 
 /*
