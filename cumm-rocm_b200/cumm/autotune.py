@@ -44,9 +44,11 @@ def _desp(dt_in, dt_out):
 
 
 def run_forward(cfg: FwdConfig, x: torch.Tensor, w: torch.Tensor, out: torch.Tensor, tables: Dict,
-                dt_in=tv.bfloat16, dt_out=tv.bfloat16, stream: int = 0, cm: ConvMainUnitTest = None):
+                dt_in=tv.bfloat16, dt_out=tv.bfloat16, stream: int = 0, cm: ConvMainUnitTest = None,
+                act_type: int = 0, scale: torch.Tensor = None):
     """Forward conv of one (possibly batched) cloud with configuration `cfg`.
-    `tables[num_split]` is the PairTable built with that split count."""
+    `tables[num_split]` is the PairTable built with that split count.
+    act_type / scale: epilogue activation and per-output-channel scale (E4M3)."""
     pt = tables[cfg.num_split]
     cm = cm or ConvMainUnitTest()
     desp = _desp(dt_in, dt_out)
@@ -61,6 +63,10 @@ def run_forward(cfg: FwdConfig, x: torch.Tensor, w: torch.Tensor, out: torch.Ten
         p.mask_filter = pt.split_masks[j] if cfg.num_split > 1 else 0xffffffff
         p.beta = 1.0 if j > 0 else 0.0
         p.tile_n = cfg.tile_n
+        if scale is not None:
+            p.scale = tv.Tensor(scale)
+        if act_type and j == cfg.num_split - 1:
+            p.act_type = act_type
         p.stream = stream or torch.cuda.current_stream().cuda_stream
         cm.implicit_gemm2(p)
 

@@ -1,0 +1,343 @@
+"""Serving a sparse-conv encoder: continuous batching of requests by HBM budget.
+
+Network (one request = one point cloud through all layers, ReLU after each):
+    subm 16->16, subm 16->16, down 16->32, subm 32->32, down 32->64,
+    subm 64->64, subm 64->64, down 64->128, subm 128->128, subm 128->128
+(submanifold 3x3x3, and 3x3x3 stride-2 pad-1 downsamples), bf16 operands with
+fp32 accumulation; with fp8=True every layer runs E4M3 operands (weights
+quantized once per output channel, activation tile scales calibrated once on a
+calibration cloud and folded into the weights, cumm.precision).
+
+Pair tables stay on the device for the whole request: consecutive
+submanifold layers at one resolution share one table, a downsample builds the
+strided table and the next resolution's coordinates.
+
+Server (continuous batching): requests wait in a FIFO.  Whenever one of the
+`slots` pass slots (a worker thread with its own CUDA stream) is free, every
+request at the head of the FIFO that has arrived and whose HBM footprint
+estimate fits in what the budget has left joins one batched pass through the
+encoder (one pair build and one conv launch per layer for all of them).
+Requests that arrive while passes run are admitted into the next pass as soon
+as a slot and memory free up, and two passes overlap on the device.  The plain
+path runs one request at a time on one stream.
+
+``python -m cumm.serve`` sweeps Poisson arrival rates (50 ... 800 req/s) with
+clouds of 10k to 400k voxels (lognormal, median 60k, sigma 0.8) and prints one
+JSON line per (rate, mode) with p50 / p99 latency and voxels/s.
+"""
+import threading
+import time
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from cumm import tensorview as tv
+from cumm.autotune import FwdConfig, run_forward
+from cumm.precision import quantize_act_fp8, quantize_weight_fp8
+from cumm.spconv_ops import build_pair_table
+
+LAYERS = (("subm", 16, 16), ("subm", 16, 16), ("down", 16, 32), ("subm", 32, 32), ("down", 32, 64),
+          ("subm", 64, 64), ("subm", 64, 64), ("down", 64, 128), ("subm", 128, 128),
+          ("subm", 128, 128))
+ACT_RELU = 1
+
+
+class SparseEncoder:
+    def __init__(self, spatial_shape: Sequence[int], layers=LAYERS, seed: int = 0,
+                 device="cuda", fp8: bool = False):
+        from cumm import voxelgen as vg
+        self.spatial = list(spatial_shape)
+        self.layers = list(layers)
+        self.dev = torch.device(device)
+        self.w = [torch.from_numpy(vg.kaiming_uniform(k, 27, c, seed + i)).to(self.dev)
+                  for i, (_, c, k) in enumerate(self.layers)]
+        self.wb = [w.bfloat16() for w in self.w]
+        self.fp8 = fp8
+        self.wq: List[torch.Tensor] = []
+        self.sw: List[torch.Tensor] = []
+        self.sx: List[torch.Tensor] = []
+
+    def calibrate(self, coords: torch.Tensor, feats: torch.Tensor):
+        """Fixes the E4M3 activation tile scales from one bf16 pass (amax of
+        every layer's input, 2x headroom) and quantizes the weights with them."""
+        acts = []
+        self.forward(coords, feats, record=acts, use_fp8=False)
+        self.wq, self.sw, self.sx = [], [], []
+        for w, (a, _, _) in zip(self.w, acts):
+            _, sx = quantize_act_fp8(a)
+            sx = sx * 2.0
+            wq, sw = quantize_weight_fp8(w, sx)
+            self.wq.append(wq)
+            self.sw.append(sw)
+            self.sx.append(sx)
+
+    def _quant_input(self, x: torch.Tensor, i: int) -> torch.Tensor:
+        s = self.sx[i].repeat_interleave(64)[: x.shape[1]]
+        return (x.float() / s[None, :]).clamp(-448.0, 448.0).to(torch.float8_e4m3fn)
+
+    def forward(self, coords: torch.Tensor, feats: torch.Tensor, record: Optional[list] = None,
+                use_fp8: Optional[bool] = None, batch_size: int = 1) -> Tuple[torch.Tensor, torch.Tensor]:
+        """Runs every layer on the current stream; returns (features, coords)
+        of the last layer (bf16, int32).  `record` collects (input, pair
+        table, output) per layer.  coords[:, 0] is the batch index (< batch_size):
+        clouds of one batch never pair with each other, submanifold rows keep
+        their order and strided outputs come out batch-major, so every cloud's
+        rows stay contiguous."""
+        fp8 = self.fp8 if use_fp8 is None else use_fp8
+        x = feats
+        cur, spatial = coords, self.spatial
+        table = None
+        for i, (kind, c, k) in enumerate(self.layers):
+            if kind == "subm":
+                if table is None:
+                    table = build_pair_table(cur, spatial)
+                pt, n_out = table, cur.shape[0]
+            else:
+                pt = build_pair_table(cur, spatial, stride=(2, 2, 2), padding=(1, 1, 1), subm=False,
+                                      batch_size=batch_size)
+                n_out = pt.n_out
+            out = torch.empty((n_out, k), dtype=torch.bfloat16, device=self.dev)
+            if fp8:
+                run_forward(FwdConfig(1, 0), self._quant_input(x, i), self.wq[i], out, {1: pt},
+                            tv.float_e4m3, tv.bfloat16, act_type=ACT_RELU, scale=self.sw[i])
+            else:
+                run_forward(FwdConfig(1, 0), x, self.wb[i], out, {1: pt}, act_type=ACT_RELU)
+            if record is not None:
+                record.append((x, pt, out))
+            x = out
+            if kind == "down":
+                cur, spatial, table = pt.out_inds, pt.out_spatial, None
+        return x, cur
+
+    @staticmethod
+    def footprint_bytes(n: int) -> int:
+        """Upper estimate of a request's device memory at n input voxels: the
+        first resolution dominates (27-offset fwd/bwd pair tables, the sorted
+        index table, masks, argsorts, hash table, 16-channel features), plus
+        one strided table; 1 KB per voxel covers it with headroom."""
+        return 1024 * n + (8 << 20)
+
+
+class Admission:
+    """HBM-budget and slot accounting (thread-safe)."""
+
+    def __init__(self, budget_bytes: int, slots: int):
+        self.budget = budget_bytes
+        self.slots = slots
+        self.used = 0
+        self.active = 0
+        self.cv = threading.Condition()
+
+    def fits(self, nbytes: int) -> bool:
+        return self.active < self.slots and self.used + nbytes <= self.budget
+
+    def try_admit(self, nbytes: int) -> bool:
+        with self.cv:
+            if nbytes > self.budget:
+                raise ValueError(f"request needs {nbytes} bytes, budget is {self.budget}")
+            if not self.fits(nbytes):
+                return False
+            self.used += nbytes
+            self.active += 1
+            return True
+
+    def release(self, nbytes: int):
+        with self.cv:
+            self.used -= nbytes
+            self.active -= 1
+            self.cv.notify_all()
+
+    def wait_change(self, timeout: float):
+        with self.cv:
+            self.cv.wait(timeout)
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float           # seconds after the start of the run
+    coords: torch.Tensor     # pinned host [n, 4] int32
+    feats: torch.Tensor      # pinned host [n, 16] bf16
+    done: float = 0.0
+    out: Optional[torch.Tensor] = None
+    out_coords: Optional[torch.Tensor] = None
+
+    @property
+    def n(self) -> int:
+        return self.coords.shape[0]
+
+
+def _run_batch(enc: SparseEncoder, reqs: Sequence[Request], stream: torch.cuda.Stream, keep: bool):
+    """One batched pass of the encoder over `reqs` on `stream` (inputs copied
+    from pinned host memory on the stream, batch index = position)."""
+    B = len(reqs)
+    with torch.cuda.stream(stream):
+        cs, fs = [], []
+        for b, r in enumerate(reqs):
+            c = r.coords.to(enc.dev, non_blocking=True)
+            c[:, 0] = b
+            cs.append(c)
+            fs.append(r.feats.to(enc.dev, non_blocking=True))
+        c = cs[0] if B == 1 else torch.cat(cs, 0)
+        x = fs[0] if B == 1 else torch.cat(fs, 0)
+        y, yc = enc.forward(c, x, batch_size=B)
+        counts = torch.bincount(yc[:, 0].long(), minlength=B) if B > 1 else None
+    stream.synchronize()
+    if keep:
+        offs = [0] + (torch.cumsum(counts, 0).tolist() if B > 1 else [y.shape[0]])
+        for b, r in enumerate(reqs):
+            r.out, r.out_coords = y[offs[b]:offs[b + 1]], yc[offs[b]:offs[b + 1]].clone()
+            r.out_coords[:, 0] = 0
+
+
+def serve(enc: SparseEncoder, requests: List[Request], continuous: bool = True,
+          budget_bytes: int = 16 << 30, slots: int = 2, max_batch: int = 64,
+          max_batch_voxels: int = 2_000_000, keep_outputs: bool = False) -> Dict:
+    """Replays `requests` at their arrival times; returns latency statistics.
+
+    continuous=False: one request at a time on one stream (the plain path).
+    continuous=True: whenever a slot is free, every arrived request at the
+    head of the FIFO that fits in the remaining HBM budget joins one batched
+    pass (at most max_batch requests and max_batch_voxels voxels, which bounds
+    one pass's latency); up to `slots` passes run at once on their own streams."""
+    reqs = sorted(requests, key=lambda r: r.arrival)
+    t0 = time.perf_counter()
+    batches = []
+    if not continuous:
+        s = torch.cuda.Stream()
+        for r in reqs:
+            now = time.perf_counter() - t0
+            if now < r.arrival:
+                time.sleep(r.arrival - now)
+            _run_batch(enc, [r], s, keep_outputs)
+            r.done = time.perf_counter() - t0
+            batches.append(1)
+    else:
+        adm = Admission(budget_bytes, slots)
+        queue = deque(reqs)
+        free_streams = deque(torch.cuda.Stream() for _ in range(slots))
+        lock = threading.Lock()
+        threads, errors = [], []
+
+        def worker(batch: List[Request], st: torch.cuda.Stream, nbytes: int):
+            try:
+                _run_batch(enc, batch, st, keep_outputs)
+                t = time.perf_counter() - t0
+                for r in batch:
+                    r.done = t
+            except Exception as e:  # surfaced after the run
+                errors.append(e)
+            finally:
+                with lock:
+                    free_streams.append(st)
+                adm.release(nbytes)
+
+        while queue:
+            now = time.perf_counter() - t0
+            if queue[0].arrival > now:
+                time.sleep(min(queue[0].arrival - now, 0.0005))
+                continue
+            # the arrived head of the FIFO, as far as the budget left allows
+            with adm.cv:
+                room = adm.budget - adm.used if adm.active < adm.slots else -1
+            batch, nbytes, nvox = [], 0, 0
+            for r in queue:
+                if r.arrival > now or len(batch) >= max_batch:
+                    break
+                if batch and nvox + r.n > max_batch_voxels:
+                    break
+                nvox += r.n
+                need = enc.footprint_bytes(r.n)
+                if need > adm.budget:
+                    raise ValueError(f"request {r.rid} needs {need} bytes, budget is {adm.budget}")
+                if nbytes + need > room:
+                    break
+                batch.append(r)
+                nbytes += need
+            if batch and adm.try_admit(nbytes):
+                for _ in batch:
+                    queue.popleft()
+                with lock:
+                    st = free_streams.popleft()
+                th = threading.Thread(target=worker, args=(batch, st, nbytes), daemon=True)
+                th.start()
+                threads.append(th)
+                batches.append(len(batch))
+            else:
+                adm.wait_change(0.0005)
+        for th in threads:
+            th.join()
+        if errors:
+            raise errors[0]
+    lat = np.array([(r.done - r.arrival) * 1e3 for r in reqs])
+    span = max(r.done for r in reqs) - min(r.arrival for r in reqs)
+    vox = sum(r.n for r in reqs)
+    return {"requests": len(reqs), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+            "voxels_per_s": vox / span, "makespan_s": span,
+            "passes": len(batches), "mean_batch": float(np.mean(batches))}
+
+
+def make_requests(n: int, rate: float, seed: int = 0, median: int = 60_000, sigma: float = 0.8,
+                  lo: int = 10_000, hi: int = 400_000, pool: Optional[List] = None) -> List[Request]:
+    """Poisson arrivals at `rate` req/s; clouds drawn from `pool` (a list of
+    (coords, feats) pinned host pairs) or generated."""
+    from cumm import voxelgen as vg
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    reqs = []
+    for i in range(n):
+        if pool is not None:
+            c, f = pool[int(rng.integers(len(pool)))]
+        else:
+            m = int(np.clip(round(median * np.exp(sigma * rng.standard_normal())), lo, hi))
+            c = torch.from_numpy(vg.lidar_voxels(m, seed=seed * 1000 + i)).pin_memory()
+            f = torch.from_numpy(rng.standard_normal((m, 16)).astype(np.float32)).bfloat16().pin_memory()
+        reqs.append(Request(i, float(t[i]), c, f))
+    return reqs
+
+
+def make_pool(k: int = 24, seed: int = 0, median: int = 60_000, sigma: float = 0.8,
+              lo: int = 10_000, hi: int = 400_000):
+    from cumm import voxelgen as vg
+    rng = np.random.default_rng(seed + 7)
+    pool = []
+    for i in range(k):
+        m = int(np.clip(round(median * np.exp(sigma * rng.standard_normal())), lo, hi))
+        c = torch.from_numpy(vg.lidar_voxels(m, seed=seed * 100 + i)).pin_memory()
+        f = torch.from_numpy(rng.standard_normal((m, 16)).astype(np.float32)).bfloat16().pin_memory()
+        pool.append((c, f))
+    return pool
+
+
+def main(rates=(50, 100, 200, 400, 800), n_req: int = 160, fp8: bool = False, seed: int = 0):
+    import json
+
+    from cumm import voxelgen as vg
+    enc = SparseEncoder(vg.KITTI_SHAPE, fp8=fp8, seed=seed)
+    pool = make_pool(seed=seed)
+    if fp8:
+        c, f = pool[0]
+        enc.calibrate(c.cuda(), f.cuda())
+    # warm-up: kernels loaded, and the allocator of both pass streams holds
+    # the buffers of full-size passes before anything is timed
+    warm = make_requests(8, 1000.0, seed + 99, pool=pool)
+    serve(enc, warm, continuous=False)
+    for _ in range(2):
+        serve(enc, make_requests(96, 5000.0, seed + 98, pool=pool), continuous=True)
+    for rate in rates:
+        for continuous in (False, True):
+            reqs = make_requests(n_req, float(rate), seed + rate, pool=pool)
+            st = serve(enc, reqs, continuous=continuous)
+            st.update({"rate_req_s": rate, "mode": "continuous" if continuous else "plain",
+                       "dtype": "e4m3" if fp8 else "bf16",
+                       "encoder": "subm16x2,down32,subm32,down64,subm64x2,down128,subm128x2"})
+            print(json.dumps(st), flush=True)
+
+
+if __name__ == "__main__":
+    import sys
+    main(fp8="--fp8" in sys.argv)
