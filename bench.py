@@ -91,6 +91,22 @@ class ClockSampler:
                 "samples": len(sms), "reasons": sorted(reasons)}
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The slowest rank's value (every rank takes part; identity at N = 1)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_tflops(flops_per_rank_step: float, world: int, ms: float) -> float:
+    """Replicas: every rank runs its own cloud, so the job does world x the
+    per-rank work in the slowest rank's time."""
+    return flops_per_rank_step * world / (ms * 1e-3) / 1e12
+
+
 def cpu_reference_step(x, w, dy, pf, pb):
     """fp32 numpy gather-GEMM-scatter fwd + dgrad + wgrad (the reference's CPU path)."""
     from oracle import conv_oracle as co
@@ -263,12 +279,8 @@ def run_b200(args, rank, world, dist):
     bits = _lib.device_error_bits(sptr)
     if bits:
         raise RuntimeError(f"device error word {bits} during timing")
-    ms_max = ms_step
-    if dist is not None:
-        t = torch.tensor([ms_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = 3 * flops_op * world / (ms_max * 1e-3) / 1e12
+    ms_max = max_over_ranks(ms_step, dist, dev)
+    value = whole_job_tflops(3 * flops_op, world, ms_max)
 
     # ---------------------------------------------------------------- end to end (public API)
     coords_h = torch.from_numpy(coords_np).pin_memory()
@@ -332,11 +344,8 @@ def run_b200(args, rank, world, dist):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / max(n_e2e, 1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = 3 * flops_op * world / (e2e_ms * 1e-3) / 1e12
+    e2e_ms = max_over_ranks(e2e_ms, dist, dev)
+    e2e_value = whole_job_tflops(3 * flops_op, world, e2e_ms)
     h2d = coords_h.numel() * 4 + x_h.numel() * 2 + dy_h.numel() * 2
     d2h = out_h.numel() * 2 + din_h.numel() * 2 + dw_h.numel() * 4
 
