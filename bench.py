@@ -11,7 +11,9 @@ fp32 accumulation: forward + backward-input + backward-weight).
 * ``e2e``: the same metric through the public API with host buffers: per step
   the pinned-host coordinates, features and upstream gradient are copied in,
   the pair table is built on the GPU, the three ops run, and output, input
-  gradient and weight gradient are copied back.
+  gradient and weight gradient are copied back.  Consecutive steps are
+  pipelined over an upload, a compute and a download stream (full-duplex
+  copies overlap the next and previous steps' compute).
 * ``cpu_baseline`` / ``--impl reference``: the reference's own CPU algorithm
   for this path (numpy gather-GEMM-scatter, cumm/conv/main_real_spconv.py:309-403)
   restated in oracle/conv_oracle.py, fp32, BLAS on all host cores.
@@ -286,64 +288,95 @@ def run_b200(args, rank, world, dist):
     coords_h = torch.from_numpy(coords_np).pin_memory()
     x_h = torch.from_numpy(x_np).bfloat16().pin_memory()
     dy_h = torch.from_numpy(dy_np).bfloat16().pin_memory()
-    out_h = torch.empty((N_VOX, K), dtype=torch.bfloat16).pin_memory()
-    din_h = torch.empty((N_VOX, C), dtype=torch.bfloat16).pin_memory()
-    dw_h = torch.empty((K, KV, C), dtype=torch.float32).pin_memory()
     from cumm.conv.main import ConvMainUnitTest
     cmt = ConvMainUnitTest()
+    # Steps are pipelined over three streams (uploads, compute, downloads):
+    # step s+1's inputs go up while step s computes and step s-1's results
+    # come down; two device and two pinned host buffer sets alternate.
+    # Every step still copies its inputs in and its results out inside the
+    # timed region.
+    s_in, s_comp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    bufs = []
+    for _ in range(2):
+        bufs.append({
+            "cd": torch.empty_like(coords_h, device=dev), "xd": torch.empty_like(x_h, device=dev),
+            "dyd": torch.empty_like(dy_h, device=dev),
+            "outd": torch.empty((N_VOX, K), dtype=torch.bfloat16, device=dev),
+            "dind": torch.empty((N_VOX, C), dtype=torch.bfloat16, device=dev),
+            "dwd": torch.empty((K, KV, C), dtype=torch.float32, device=dev),
+            "mod": torch.empty(((N_VOX + 127) // 128,), dtype=torch.int32, device=dev),
+            "out_h": torch.empty((N_VOX, K), dtype=torch.bfloat16).pin_memory(),
+            "din_h": torch.empty((N_VOX, C), dtype=torch.bfloat16).pin_memory(),
+            "dw_h": torch.empty((K, KV, C), dtype=torch.float32).pin_memory(),
+            "ev_in": torch.cuda.Event(), "ev_fwd": torch.cuda.Event(),
+            "ev_done": torch.cuda.Event(), "ev_free": torch.cuda.Event(),
+        })
 
-    def e2e_step():
-        cd = coords_h.to(dev, non_blocking=True)
-        xd = x_h.to(dev, non_blocking=True)
-        dyd = dy_h.to(dev, non_blocking=True)
-        ptd = build_pair_table(cd, vg.KITTI_SHAPE)
-        outd = torch.empty((N_VOX, K), dtype=torch.bfloat16, device=dev)
-        dind = torch.empty((N_VOX, C), dtype=torch.bfloat16, device=dev)
-        dwd = torch.empty((K, KV, C), dtype=torch.float32, device=dev)
-        mod = torch.empty(((N_VOX + 127) // 128,), dtype=torch.int32, device=dev)
-        for op in (ConvOpType.kForward, ConvOpType.kBackwardInput, ConvOpType.kBackwardWeight):
-            p = ConvParams(3, op)
-            p.conv_algo_desp = desp_for(op, tv.float32 if op == ConvOpType.kBackwardWeight
-                                        else tv.bfloat16)
-            if op == ConvOpType.kForward:
-                p.input, p.weight, p.output = tv.Tensor(xd), tv.Tensor(w), tv.Tensor(outd)
-                p.indices = tv.Tensor(ptd.pairs_fwd)
-                p.mask = tv.Tensor(ptd.masks_fwd[0], tv.uint32)
-                p.mask_output = tv.Tensor(mod, tv.uint32)
-            elif op == ConvOpType.kBackwardInput:
-                p.input, p.weight, p.output = tv.Tensor(dind), tv.Tensor(w), tv.Tensor(dyd)
-                p.indices = tv.Tensor(ptd.pairs_bwd)
-                p.mask = tv.Tensor(ptd.masks_fwd[0], tv.uint32)
-                p.reverse_mask = True
-            else:
-                p.input, p.weight, p.output = tv.Tensor(xd), tv.Tensor(dwd), tv.Tensor(dyd)
-                p.indices = tv.Tensor(ptd.pairs_fwd)
-                p.mask = tv.Tensor(mod, tv.uint32)
-                p.mask_width = 128
-            p.mask_argsort = tv.Tensor(ptd.argsorts_fwd[0])
-            p.indices_sorted = tv.Tensor(ptd.sorted_indices(
-                "bwd" if op == ConvOpType.kBackwardInput else "fwd"))
-            p.stream = sptr
-            cmt.implicit_gemm2(p)
-        out_h.copy_(outd, non_blocking=True)
-        din_h.copy_(dind, non_blocking=True)
-        dw_h.copy_(dwd, non_blocking=True)
-        torch.cuda.synchronize()
+    def e2e_step(step: int):
+        b = bufs[step % 2]
+        with torch.cuda.stream(s_in):
+            if step >= 2:
+                s_in.wait_event(b["ev_free"])
+            b["cd"].copy_(coords_h, non_blocking=True)
+            b["xd"].copy_(x_h, non_blocking=True)
+            b["dyd"].copy_(dy_h, non_blocking=True)
+            b["ev_in"].record(s_in)
+        with torch.cuda.stream(s_comp):
+            s_comp.wait_event(b["ev_in"])
+            if step >= 2:
+                s_comp.wait_event(b["ev_free"])
+            cptr = s_comp.cuda_stream
+            ptd = build_pair_table(b["cd"], vg.KITTI_SHAPE)
+            for op in (ConvOpType.kForward, ConvOpType.kBackwardInput, ConvOpType.kBackwardWeight):
+                p = ConvParams(3, op)
+                p.conv_algo_desp = desp_for(op, tv.float32 if op == ConvOpType.kBackwardWeight
+                                            else tv.bfloat16)
+                if op == ConvOpType.kForward:
+                    p.input, p.weight, p.output = tv.Tensor(b["xd"]), tv.Tensor(w), tv.Tensor(b["outd"])
+                    p.indices = tv.Tensor(ptd.pairs_fwd)
+                    p.mask = tv.Tensor(ptd.masks_fwd[0], tv.uint32)
+                    p.mask_output = tv.Tensor(b["mod"], tv.uint32)
+                elif op == ConvOpType.kBackwardInput:
+                    p.input, p.weight, p.output = tv.Tensor(b["dind"]), tv.Tensor(w), tv.Tensor(b["dyd"])
+                    p.indices = tv.Tensor(ptd.pairs_bwd)
+                    p.mask = tv.Tensor(ptd.masks_fwd[0], tv.uint32)
+                    p.reverse_mask = True
+                else:
+                    p.input, p.weight, p.output = tv.Tensor(b["xd"]), tv.Tensor(b["dwd"]), tv.Tensor(b["dyd"])
+                    p.indices = tv.Tensor(ptd.pairs_fwd)
+                    p.mask = tv.Tensor(b["mod"], tv.uint32)
+                    p.mask_width = 128
+                p.mask_argsort = tv.Tensor(ptd.argsorts_fwd[0])
+                p.indices_sorted = tv.Tensor(ptd.sorted_indices(
+                    "bwd" if op == ConvOpType.kBackwardInput else "fwd"))
+                p.stream = cptr
+                cmt.implicit_gemm2(p)
+                if op == ConvOpType.kForward:
+                    b["ev_fwd"].record(s_comp)
+            b["ev_done"].record(s_comp)
+        with torch.cuda.stream(s_out):
+            s_out.wait_event(b["ev_fwd"])
+            b["out_h"].copy_(b["outd"], non_blocking=True)
+            s_out.wait_event(b["ev_done"])
+            b["din_h"].copy_(b["dind"], non_blocking=True)
+            b["dw_h"].copy_(b["dwd"], non_blocking=True)
+            b["ev_free"].record(s_out)
 
     n_e2e = 0 if args.no_e2e else max(3, min(args.steps, 20))
-    for _ in range(2 if n_e2e else 0):
-        e2e_step()
+    for st in range(2 if n_e2e else 0):
+        e2e_step(st)
+    torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-    torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(n_e2e):
-        e2e_step()
-    e1.record(stream)
+    e0.record(s_in)
+    for st in range(n_e2e):
+        e2e_step(st)
+    e1.record(s_out)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / max(n_e2e, 1)
+    out_h, din_h, dw_h = bufs[0]["out_h"], bufs[0]["din_h"], bufs[0]["dw_h"]
     e2e_ms = max_over_ranks(e2e_ms, dist, dev)
     e2e_value = whole_job_tflops(3 * flops_op, world, e2e_ms)
     h2d = coords_h.numel() * 4 + x_h.numel() * 2 + dy_h.numel() * 2
@@ -396,7 +429,8 @@ def run_b200(args, rank, world, dist):
             "roofline": roofline,
             "e2e": None if n_e2e == 0 else {
                 "value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                "steps": n_e2e, "pipelined_streams": 3},
             "cpu_baseline": cpu,
             "gpu_launches": 5 * args.steps,
             "clocks": clocks,
