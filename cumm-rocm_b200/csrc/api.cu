@@ -105,8 +105,13 @@ bool rowgather_width_ok(int64_t bytes) {
 
 struct ConvPlan {
   bool simt = false;
-  int64_t ws_bytes = 0;
+  int64_t ws_bytes = 0;  // what sc_conv_workspace_size reports
+  int64_t ws_min = 0;    // what a call cannot run without
 };
+
+// Workspace head of the tcgen05 forward / backward-input kernels: the tile
+// counter of their dynamic scheduler (zeroed per call).
+constexpr int64_t kSchedBytes = 256;
 
 int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
   if (p == nullptr) return fail(SC_INVALID_ARG, "params is null");
@@ -160,7 +165,7 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
       return fail(SC_RUNTIME, "Can't Found Algorithm: Simt kernels take float32 operands (%s %s %s)",
                   dtype_name(di), dtype_name(dw), dtype_name(dout));
     plan->simt = true;
-    if (op == SC_CONV_BACKWARD_WEIGHT) plan->ws_bytes = align256(p->K * p->kv * p->C * 4);
+    if (op == SC_CONV_BACKWARD_WEIGHT) plan->ws_bytes = plan->ws_min = align256(p->K * p->kv * p->C * 4);
     return SC_OK;
   }
   if (p->algo != SC_ALGO_TCGEN05) return fail(SC_RUNTIME, "Can't Found Algorithm: unknown algo %d", p->algo);
@@ -180,6 +185,7 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
       return fail(SC_RUNTIME, "Can't Found Algorithm: C=%lld K=%lld not tiled by the tcgen05 kernel "
                   "(C*sizeof in {16,32,64} or a multiple of 16 >= 128 bytes; K %% 16 == 0)",
                   (long long)p->C, (long long)p->K);
+    plan->ws_bytes = kSchedBytes;  // optional: without it tiles are dealt statically
     return SC_OK;
   }
   if (op == SC_CONV_BACKWARD_INPUT) {
@@ -189,7 +195,8 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
     if (!rowgather_width_ok(p->K * esize(di)) || p->C % 16)
       return fail(SC_RUNTIME, "Can't Found Algorithm: K=%lld C=%lld not tiled by the tcgen05 kernel",
                   (long long)p->K, (long long)p->C);
-    plan->ws_bytes = align256(p->K * p->kv * p->C * esize(di));
+    plan->ws_bytes = kSchedBytes + align256(p->K * p->kv * p->C * esize(di));
+    plan->ws_min = plan->ws_bytes;
     return SC_OK;
   }
   // backward weight
@@ -200,6 +207,7 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
     return fail(SC_RUNTIME, "Can't Found Algorithm: C=%lld K=%lld not tiled by the tcgen05 wgrad kernel",
                 (long long)p->C, (long long)p->K);
   plan->ws_bytes = align256(p->K * p->kv * p->C * 4);
+  plan->ws_min = plan->ws_bytes;
   return SC_OK;
 }
 
@@ -276,8 +284,8 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
   ConvPlan plan;
   int rc = plan_conv(p, &plan);
   if (rc != SC_OK) return rc;
-  if (plan.ws_bytes > 0 && (p->workspace == nullptr || p->workspace_bytes < plan.ws_bytes))
-    return fail(SC_RUNTIME, "workspace at least %lld bytes.", (long long)plan.ws_bytes);
+  if (plan.ws_min > 0 && (p->workspace == nullptr || p->workspace_bytes < plan.ws_min))
+    return fail(SC_RUNTIME, "workspace at least %lld bytes.", (long long)plan.ws_min);
   int *err = nullptr;
   int sms = 0;
   rc = device_state(&err, &sms);
@@ -345,6 +353,12 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     const int64_t red = fwd ? p->C : p->K;    // reduction elements per offset
     const int64_t ncols = fwd ? p->K : p->C;  // output columns
     scb::ConvRowGatherArgs a{};
+    uint8_t *ws = static_cast<uint8_t *>(p->workspace);
+    if (ws != nullptr && p->workspace_bytes >= plan.ws_bytes) {
+      e = cudaMemsetAsync(ws, 0, sizeof(int), s);
+      if (e != cudaSuccess) return cuda_fail(e, "zero tile counter");
+      a.tile_counter = reinterpret_cast<int *>(ws);
+    }
     a.a_base = static_cast<const uint8_t *>(fwd ? p->input : p->output);
     a.a_rows = fwd ? p->n_in : p->n_out;
     a.a_row_bytes = static_cast<int>(red * es);
@@ -352,10 +366,10 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     if (fwd) {
       a.b_base = static_cast<const uint8_t *>(p->weight);
     } else {
-      e = scb::launch_transpose_weight(p->weight, p->workspace, static_cast<int>(p->K), p->kv,
+      e = scb::launch_transpose_weight(p->weight, ws + kSchedBytes, static_cast<int>(p->K), p->kv,
                                        static_cast<int>(p->C), es, s);
       if (e != cudaSuccess) return cuda_fail(e, "weight transpose launch");
-      a.b_base = static_cast<const uint8_t *>(p->workspace);
+      a.b_base = ws + kSchedBytes;
     }
     a.b_row_stride = static_cast<int64_t>(p->kv) * red * es;
     a.b_off_stride = static_cast<int>(red * es);

@@ -50,7 +50,7 @@ struct Meta {
   int nchunks;
   int n_active;
   uint32_t tilemask;
-  uint32_t pad;
+  int tile;  // tile index of this ring slot, -1 = no more tiles
   uint32_t grp[4];
   int k_list[32];
 };
@@ -186,8 +186,12 @@ __global__ void __maxnreg__(96)
   uint64_t *acc_full = idx_empty + kIdxStages;
   uint64_t *acc_empty = acc_full + 2;
   uint64_t *drain_bar = acc_empty + 2;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain_bar + 1);
+  uint64_t *tile_bar = drain_bar + 1;  // [2]: tile of accumulator buffer b announced
+  uint64_t *sched_bar = tile_bar + 2;  // [4]: next tile drawn by loader warp 0
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sched_bar + 4);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  volatile int *acc_tile = abort_flag + 1;    // [2]: tile held by accumulator buffer b
+  volatile int *sched_tile = acc_tile + 2;    // [4]: tile of loader iteration i (slot i & 3)
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -210,6 +214,9 @@ __global__ void __maxnreg__(96)
       mbar_init(&acc_empty[i], 128);
     }
     mbar_init(drain_bar, 1);
+    mbar_init(&tile_bar[0], 1);
+    mbar_init(&tile_bar[1], 1);
+    for (int i = 0; i < 4; ++i) mbar_init(&sched_bar[i], 1);
     *abort_flag = 0;
     fence_mbar_init();
   }
@@ -226,8 +233,7 @@ __global__ void __maxnreg__(96)
     // ---------------------------------------------------------------- index loaders
     const int r = threadIdx.x - kLoadWarp0 * 32;  // row inside the tile
     const int lw = r >> 5;
-    int it = 0;
-    for (int tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
+    for (int it = 0;; ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
       if (!mbar_wait(&idx_empty[b], ph ^ 1, abort_flag)) {
@@ -237,6 +243,38 @@ __global__ void __maxnreg__(96)
       uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
       int *tab = reinterpret_cast<int *>(buf);
       Meta *meta = reinterpret_cast<Meta *>(buf + A.kv * kTileM * 4);
+      // Next tile: from the launch-wide counter when there is one (CTAs that
+      // drew small tiles come back for more, which evens out the per-CTA
+      // work), else every gridDim.x-th tile.  Lane 0 of loader warp 0 draws
+      // it and publishes it through slot it & 3 (store, then arrive); the
+      // other loader warps take it with a bounded wait.  A reader can trail
+      // the drawer by two iterations at most (the drawer's idx_empty wait for
+      // iteration i + 2 needs every loader thread's idx_full arrival for
+      // i - 1), so four slots are never overwritten before they are read.
+      int tile;
+      if (lw == 0) {
+        int t = -1;
+        if (lane == 0) {
+          const int64_t d = A.tile_counter
+                                ? static_cast<int64_t>(atomicAdd(A.tile_counter, 1))
+                                : static_cast<int64_t>(blockIdx.x) + static_cast<int64_t>(it) * gridDim.x;
+          t = d < P.num_tiles ? static_cast<int>(d) : -1;
+          sched_tile[it & 3] = t;
+          mbar_arrive(&sched_bar[it & 3]);
+        }
+        tile = __shfl_sync(0xffffffffu, t, 0);
+      } else {
+        if (!mbar_wait(&sched_bar[it & 3], (it >> 2) & 1, abort_flag)) {
+          flag_error(A.err, kErrWaitTimeout);
+          break;
+        }
+        tile = sched_tile[it & 3];
+      }
+      if (tile < 0) {
+        if (r == 0) meta->tile = -1;
+        mbar_arrive(&idx_full[b]);
+        break;
+      }
       const int64_t tile_m = tile / A.n_tiles;
       const int n_tile = static_cast<int>(tile % A.n_tiles);
       const int64_t row_g = tile_m * kTileM + r;
@@ -328,6 +366,7 @@ __global__ void __maxnreg__(96)
         }
         meta->n_active = na;
         meta->tilemask = tm;
+        meta->tile = tile;
         meta->nchunks = P.cpo > 0 ? na * P.cpo : (na + P.opc - 1) / P.opc;
       }
       mbar_arrive(&idx_full[b]);
@@ -354,7 +393,7 @@ __global__ void __maxnreg__(96)
     int it = 0;
     uint32_t stage = 0, eph = 0, gchunk = 0;
     bool ok = true;
-    for (int tile = blockIdx.x; tile < P.num_tiles && ok; tile += gridDim.x, ++it) {
+    for (; ok; ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
       if (!__all_sync(0xffffffffu, mbar_wait(&idx_full[b], ph, abort_flag))) {
@@ -364,6 +403,8 @@ __global__ void __maxnreg__(96)
       const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
       const int *tab = reinterpret_cast<const int *>(buf);
       const Meta *meta = reinterpret_cast<const Meta *>(buf + A.kv * kTileM * 4);
+      const int tile = meta->tile;
+      if (tile < 0) break;
       const int nch = meta->nchunks;
       const int n0 = (tile % A.n_tiles) * A.BN;
       for (int j = 0; j < nch; ++j) {
@@ -420,7 +461,7 @@ __global__ void __maxnreg__(96)
     int it = 0;
     uint32_t c_base = 0;  // chunks of all previous tiles
     bool ok = pw < S;
-    for (int tile = blockIdx.x; tile < P.num_tiles && ok; tile += gridDim.x, ++it) {
+    for (; ok; ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
       int w_ok = 1;
@@ -433,6 +474,8 @@ __global__ void __maxnreg__(96)
       const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
       const int *tab = reinterpret_cast<const int *>(buf);
       const Meta *meta = reinterpret_cast<const Meta *>(buf + A.kv * kTileM * 4);
+      const int tile = meta->tile;
+      if (tile < 0) break;
       const int nch = meta->nchunks;
       const int na = meta->n_active;
       const int n0 = (tile % A.n_tiles) * A.BN;
@@ -533,7 +576,7 @@ __global__ void __maxnreg__(96)
       uint32_t stage = 0, fph = 0;
       bool issued = false;
       const uint64_t a_desc0 = make_sdesc(smem_base, 16, 1024);
-      for (int tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
+      for (;; ++it) {
         const int b = it % kIdxStages;
         const uint32_t ph = (it / kIdxStages) & 1;
         if (!mbar_wait(&idx_full[b], ph, abort_flag)) {
@@ -543,6 +586,7 @@ __global__ void __maxnreg__(96)
         const Meta *meta =
             reinterpret_cast<const Meta *>(smem + P.idx_off + b * P.idx_buf_bytes + A.kv * kTileM * 4);
         const int nch = meta->nchunks;
+        const int tile = meta->tile;
         mbar_arrive(&idx_empty[b]);
         const int ab = it & 1;
         const uint32_t aph = (it >> 1) & 1;
@@ -551,6 +595,11 @@ __global__ void __maxnreg__(96)
           break;
         }
         tc_fence_after();
+        // announce the buffer's tile to the epilogue (the plain arrive
+        // releases the store to the epilogue's wait); -1 ends the epilogue
+        acc_tile[ab] = tile;
+        mbar_arrive(&tile_bar[ab]);
+        if (tile < 0) break;
         const uint32_t d = tmem_base + static_cast<uint32_t>(ab * A.BN);
         if (nch == 0) {
           mbar_arrive(&acc_full[ab]);
@@ -598,9 +647,16 @@ __global__ void __maxnreg__(96)
   } else if (warp < kEpiWarps) {
     // ---------------------------------------------------------------- epilogue (warps 0-3)
     const int r = threadIdx.x;  // TMEM lane == tile row
-    int it = 0;
     const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
-    for (int tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x, ++it) {
+    for (int it = 0;; ++it) {
+      const int ab = it & 1;
+      const uint32_t aph = (it >> 1) & 1;
+      if (!mbar_wait(&tile_bar[ab], aph, abort_flag)) {
+        flag_error(A.err, kErrWaitTimeout);
+        break;
+      }
+      const int tile = acc_tile[ab];
+      if (tile < 0) break;
       const int64_t tile_m = tile / A.n_tiles;
       const int n0 = static_cast<int>(tile % A.n_tiles) * A.BN;
       const int64_t row_g = tile_m * kTileM + r;
@@ -616,8 +672,6 @@ __global__ void __maxnreg__(96)
 #pragma unroll
       for (int s = 16; s > 0; s >>= 1) km |= __shfl_xor_sync(0xffffffffu, km, s);
       km &= A.mask_filter;
-      const int ab = it & 1;
-      const uint32_t aph = (it >> 1) & 1;
       if (!mbar_wait(&acc_full[ab], aph, abort_flag)) {
         flag_error(A.err, kErrWaitTimeout);
         break;

@@ -51,6 +51,7 @@ struct ConvRowGatherArgs {
   const int32_t *a_inds;
   int64_t out_rows;          // bound for output rows
   const int32_t *idx_sorted; // optional [kv, M]: indices[k][argsort[r]]
+  int *tile_counter;         // optional, zero at launch: tiles handed out dynamically
 };
 cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaStream_t stream);
 

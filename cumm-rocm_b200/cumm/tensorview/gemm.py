@@ -273,18 +273,20 @@ class ConvAlgoDesp(GemmAlgoDesp):
 
     def query_conv_workspace_size(self, m: int, n: int, k: int, split_k_slices: int,
                                   kv: int) -> int:
-        """Bytes of workspace the sm_100a conv kernels need: backward-input
-        stages the weight transposed ([C, kv, K]); backward-weight accumulates
-        dW in fp32 ([K, kv, C]); forward needs none."""
+        """Bytes of workspace the sm_100a conv kernels use: the tensor-core
+        forward and backward-input kernels keep a 256-byte tile counter for
+        their dynamic scheduler (forward runs without it, dealing tiles
+        statically); backward-input also stages the weight transposed
+        ([C, kv, K]); backward-weight accumulates dW in fp32 ([K, kv, C])."""
         from . import itemsize_of
         if self.op_type == ConvOpType.kForward:
-            return 0
+            return 0 if self.algo in SIMT_ALGOS else 256
         if self.op_type == ConvOpType.kBackwardInput:
             # mnk = (N, C, K * kv)
             C, K = n, k // kv
             if self.algo in SIMT_ALGOS:
                 return 0
-            return _a256(K * kv * C * itemsize_of(self.dtype_a))
+            return 256 + _a256(K * kv * C * itemsize_of(self.dtype_a))
         # mnk = (K, C * kv, N)
         K, C = m, n // kv
         return _a256(K * kv * C * 4)

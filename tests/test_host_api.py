@@ -58,9 +58,9 @@ def _ws(cp):
 
 
 def test_conv_validation_codes():
-    assert _ws(_fake_conv())[:2] == (0, 0)
+    assert _ws(_fake_conv())[:2] == (0, 256)          # fwd: tile counter (optional)
     rc, n, _ = _ws(_fake_conv(1))
-    assert rc == 0 and n == 64 * 27 * 64 * 2          # dgrad: transposed weight
+    assert rc == 0 and n == 256 + 64 * 27 * 64 * 2    # dgrad: tile counter + transposed weight
     rc, n, _ = _ws(_fake_conv(2))
     assert rc == 0 and n == 64 * 27 * 64 * 4          # wgrad: fp32 accumulation
     rc, _, msg = _ws(_fake_conv(0, N=999))
