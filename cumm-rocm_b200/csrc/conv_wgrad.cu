@@ -69,6 +69,13 @@ struct WParams {
 
 __device__ __forceinline__ void flag_error(int *err, int bits) { atomicOr(err, bits); }
 
+// Four consecutive fp32 atomic adds (address 16-byte aligned).
+__device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, float d) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c),
+               "f"(d)
+               : "memory");
+}
+
 // Filter and channel of element e (0..63) of atom a.
 __device__ __forceinline__ void atom_elem(const WParams &P, int a, int e, int &k, int &c) {
   if (P.cpa > 0) {
@@ -521,29 +528,42 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
     }
   } else if (warp < kEpiWarps) {
     // ---------------------------------------------------------------- epilogue (warps 0-3)
+    // TMEM lane m (= threadIdx.x) holds M element m of every tile; each warp
+    // turns its 32 lanes x 32 columns through a private shared-memory tile
+    // (the stage buffers are idle once the MMA warp drained), so that a lane
+    // then owns 4 consecutive channels of one column and adds them with one
+    // red.global.add.v4.f32 (a quarter of the scalar atomics).  Only
+    // __syncwarp is used: a warp whose wait ran out never strands the others.
     if (mbar_wait(acc_full, 0, abort_flag)) {
       tc_fence_after();
       const uint32_t used = *reinterpret_cast<volatile uint32_t *>(used_tiles);
-      const int m = threadIdx.x;  // TMEM lane = M element
-      const int h = m >> 6;
-      const int e = m & 63;
       const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
+      float *tb = reinterpret_cast<float *>(smem) + warp * (32 * 33);
+      const int h = warp >> 1;               // atom of this warp's 32 M elements
+      const int e_base = (warp & 1) * 32;    // first element of the warp inside the atom
       for (int j = 0; j < t1 - t0; ++j) {
         if (!((used >> j) & 1u)) continue;
         const int a = 2 * (t0 + j) + h;
-        int k = 0, ch = 0;
-        if (a < P.n_atoms) atom_elem(P, a, e, k, ch);
-        const bool ok = a < P.n_atoms && k < A.kv && ((A.mask_filter >> k) & 1u);
         for (int n0 = 0; n0 < P.n_mma; n0 += 32) {
           float v[32];
           tmem_ld32(tmem_base + lane_base + static_cast<uint32_t>(j * P.n_mma + n0), v);
-          if (ok) {
 #pragma unroll
-            for (int i = 0; i < 32; ++i) {
-              const int n = n0 + i;
-              if (n < A.K) atomicAdd(A.ws + (static_cast<int64_t>(n) * A.kv + k) * A.C + ch, v[i]);
+          for (int i = 0; i < 32; ++i) tb[i * 33 + lane] = v[i];
+          __syncwarp();
+          const int n = n0 + lane;
+          if (a < P.n_atoms && n < A.K) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              int k = 0, ch = 0;
+              atom_elem(P, a, e_base + 4 * q, k, ch);
+              if (k < A.kv && ((A.mask_filter >> k) & 1u)) {
+                const float *src = tb + lane * 33 + 4 * q;
+                red_add_v4(A.ws + (static_cast<int64_t>(n) * A.kv + k) * A.C + ch, src[0], src[1],
+                           src[2], src[3]);
+              }
             }
           }
+          __syncwarp();
         }
       }
     } else {
