@@ -225,10 +225,20 @@ def _desp(op: ConvOpType, algo: str, dt_in: int, dt_w: int, dt_out: int, tile: T
     return d
 
 
+_ALL_CONV_DESPS: List[ConvAlgoDesp] = []
+
+
 def get_all_conv_algo_desp() -> List[ConvAlgoDesp]:
     """Every conv algorithm this build serves.  tile_shape[0] is the mask
     granularity (rows OR-ed into one mask word; 32, 64 or 128); the tcgen05
-    kernels always compute 128-row tiles and gate rows by their sub-tile's mask."""
+    kernels always compute 128-row tiles and gate rows by their sub-tile's mask.
+    Built once; callers get their own list."""
+    if not _ALL_CONV_DESPS:
+        _ALL_CONV_DESPS.extend(_build_conv_algo_desps())
+    return list(_ALL_CONV_DESPS)
+
+
+def _build_conv_algo_desps() -> List[ConvAlgoDesp]:
     res: List[ConvAlgoDesp] = []
     bf16, f16, f32, e4m3 = tv.bfloat16, tv.float16, tv.float32, tv.float_e4m3
     for tm in (128, 64, 32):
