@@ -71,6 +71,7 @@ struct KParams {
   uint32_t bar_off;
   uint32_t tmem_cols;
   uint32_t idesc;
+  int row_bytes;  // bytes of one operand row in a stage: 128 (SWIZZLE_128B) or 64 (SWIZZLE_64B)
 };
 
 __device__ __forceinline__ void flag_error(int *err, int bits) { atomicOr(err, bits); }
@@ -386,9 +387,10 @@ __global__ void __maxnreg__(96)
     // (Measured on B200: 8 warps of gather4 fill a 16 KB stage in ~740
     // cycles; per-thread cp.async arrivals serialise on the barrier word.)
     const int esz = kF8 ? 1 : 2;
-    const int box = 128 / esz;
-    const uint32_t a_tx = (kTileM / kProdWarps) * 128u;
-    const uint32_t b_tx = static_cast<uint32_t>(A.BN) * 128;
+    const int rb = P.row_bytes;  // 128, or 64 for 64-byte rows (SWIZZLE_64B stages)
+    const int box = rb / esz;
+    const uint32_t a_tx = (kTileM / kProdWarps) * static_cast<uint32_t>(rb);
+    const uint32_t b_tx = static_cast<uint32_t>(A.BN) * rb;
     const int r0 = pw * (kTileM / kProdWarps) + lane * 4;
     int it = 0;
     uint32_t stage = 0, eph = 0, gchunk = 0;
@@ -430,7 +432,7 @@ __global__ void __maxnreg__(96)
         __syncwarp();
         if (lane < (kTileM / kProdWarps) / 4) {
           const int4 q = *reinterpret_cast<const int4 *>(tab + k * kTileM + r0);
-          tma_gather4(sA + r0 * 128, &P.tmap_a, cb * box, q.x, q.y, q.z, q.w, &full_bar[s]);
+          tma_gather4(sA + r0 * rb, &P.tmap_a, cb * box, q.x, q.y, q.z, q.w, &full_bar[s]);
         }
         ++gchunk;
         if (++stage == static_cast<uint32_t>(S)) {
@@ -575,7 +577,11 @@ __global__ void __maxnreg__(96)
       int it = 0;
       uint32_t stage = 0, fph = 0;
       bool issued = false;
-      const uint64_t a_desc0 = make_sdesc(smem_base, 16, 1024);
+      // 8-row swizzle atoms: 1024 bytes apart for 128-byte rows (SWIZZLE_128B),
+      // 512 for 64-byte rows (SWIZZLE_64B); one MMA per 32 bytes of K
+      const uint64_t a_desc0 = P.row_bytes == 64 ? make_sdesc_l(smem_base, 16, 512, 4u)
+                                                 : make_sdesc(smem_base, 16, 1024);
+      const int mmas = P.row_bytes / 32;
       for (;; ++it) {
         const int b = it % kIdxStages;
         const uint32_t ph = (it / kIdxStages) & 1;
@@ -618,7 +624,8 @@ __global__ void __maxnreg__(96)
           const uint64_t bd0 = ad0 + static_cast<uint64_t>(P.b_off >> 4);
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk) {
-            // K advances 32 bytes inside the SWIZZLE_128B atom (start address >> 4)
+            if (kk >= mmas) break;
+            // K advances 32 bytes inside the swizzle atom (start address >> 4)
             const uint64_t ad = ad0 + static_cast<uint64_t>(kk * 2);
             const uint64_t bd = bd0 + static_cast<uint64_t>(kk * 2);
             if constexpr (kF8)
@@ -723,7 +730,25 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
   P.a = a;
   const int64_t m_tiles = (a.M + kTileM - 1) / kTileM;
   P.num_tiles = m_tiles * a.n_tiles;
-  if (a.a_row_bytes >= 128 || a.kv == 1) {
+  const int esz = a.in_dtype == 14 ? 1 : 2;
+  const uint64_t red = static_cast<uint64_t>(a.a_row_bytes) / esz;
+  // 64-byte rows (C = 64 e4m3, C = 32 bf16 / f16): one offset per stage in
+  // SWIZZLE_64B layout, filled by TMA gather4 like the 128-byte case, when
+  // both tensor maps encode; otherwise offsets are packed into 128-byte rows
+  // and filled with cp.async
+  bool tma = false, gather = false;
+  P.row_bytes = 128;
+  if (a.a_row_bytes == 64 && a.kv > 1 && a.a_rows > 0 &&
+      encode_tmap_2d(&P.tmap_b, a.in_dtype, a.b_base, red * a.kv, a.n_total,
+                     static_cast<uint64_t>(a.b_row_stride), 64u / esz, a.BN, 64) &&
+      encode_tmap_2d(&P.tmap_a, a.in_dtype, a.a_base, red, static_cast<uint64_t>(a.a_rows),
+                     static_cast<uint64_t>(a.a_row_stride), 64u / esz, 1, 64)) {
+    tma = gather = true;
+    P.row_bytes = 64;
+    P.cpo = 1;
+    P.opc = 1;
+    P.upo = 4;
+  } else if (a.a_row_bytes >= 128 || a.kv == 1) {
     P.cpo = (a.a_row_bytes + 127) / 128;
     P.opc = 1;
     P.upo = 8;
@@ -732,8 +757,8 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
     P.opc = 128 / a.a_row_bytes;
     P.upo = a.a_row_bytes / 16;
   }
-  const uint32_t a_bytes = kTileM * 128;
-  const uint32_t b_bytes = static_cast<uint32_t>(a.BN) * 128;
+  const uint32_t a_bytes = kTileM * static_cast<uint32_t>(P.row_bytes);
+  const uint32_t b_bytes = static_cast<uint32_t>(a.BN) * P.row_bytes;
   P.stage_bytes = a_bytes + b_bytes;
   P.b_off = a_bytes;
   P.idx_buf_bytes = ((static_cast<uint32_t>(a.kv) * kTileM * 4 + sizeof(Meta)) + 127u) & ~127u;
@@ -753,11 +778,8 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
   if (P.num_tiles == 0) return cudaSuccess;
   const int grid = static_cast<int>(P.num_tiles < num_sms ? P.num_tiles : num_sms);
   // TMA weight slabs: whole 128-byte reduction chunks (no packing of small offsets)
-  bool tma = false, gather = false;
-  if (P.cpo > 0) {
-    const int esz = a.in_dtype == 14 ? 1 : 2;
+  if (P.cpo > 0 && P.row_bytes == 128) {
     const uint32_t box = 128u / esz;
-    const uint64_t red = static_cast<uint64_t>(a.a_row_bytes) / esz;
     tma = encode_tmap_2d(&P.tmap_b, a.in_dtype, a.b_base, red * a.kv, a.n_total,
                          static_cast<uint64_t>(a.b_row_stride), box, a.BN);
     // gathered A rows: [a_rows, red] with one-row boxes (tile::gather4)

@@ -12,7 +12,8 @@ namespace scb {
 // tensor (row stride in bytes) with a box of box_outer rows x 128 bytes.
 // Returns false when TMA cannot describe the tensor (alignment, sizes).
 bool encode_tmap_2d(void *out_map, int dtype, const void *base, uint64_t inner, uint64_t outer,
-                    uint64_t row_stride_bytes, uint32_t box_inner, uint32_t box_outer);
+                    uint64_t row_stride_bytes, uint32_t box_inner, uint32_t box_outer,
+                    int swizzle_bytes = 128);
 
 // ------------------------------------------------------------------ conv fwd / dgrad (tcgen05)
 // Row-gather implicit GEMM: for every 128-row tile of the sorted row order,

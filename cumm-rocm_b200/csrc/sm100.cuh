@@ -216,17 +216,23 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
 //   bits [61,64) layout: 0 none, 2 SWIZZLE_128B, 4 SWIZZLE_64B, 6 SWIZZLE_32B
 // K-major SWIZZLE_128B operand: 8-row x 128-byte atoms, SBO = distance between
 // 8-row groups (1024 for packed rows); K advances inside an atom by moving the
-// start address 32 bytes per 16 bf16 / 32 e4m3 elements.
+// start address 32 bytes per 16 bf16 / 32 e4m3 elements.  K-major
+// SWIZZLE_64B (layout 4): 8-row x 64-byte atoms, SBO = 512 for packed rows.
 // MN-major SWIZZLE_128B operand: atoms of 64 (bf16) MN-elements x 8 K-rows;
 // LBO = distance between MN atoms, SBO = distance between 8-row K groups.
-__device__ __forceinline__ uint64_t make_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+__device__ __forceinline__ uint64_t make_sdesc_l(uint32_t saddr, uint32_t lbo, uint32_t sbo,
+                                                uint32_t layout) {
   uint64_t d = 0;
   d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
   d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
   d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
   d |= static_cast<uint64_t>(1) << 46;
-  d |= static_cast<uint64_t>(2) << 61;  // SWIZZLE_128B
+  d |= static_cast<uint64_t>(layout & 7u) << 61;
   return d;
+}
+// SWIZZLE_128B operand (the common case).
+__device__ __forceinline__ uint64_t make_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return make_sdesc_l(saddr, lbo, sbo, 2u);
 }
 
 // Instruction descriptor, kind::f16 / kind::f8f6f4 dense, fp32 accumulator.
