@@ -435,6 +435,7 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     a.b_inds = nullptr;
     a.idx_sorted = p->indices_sorted;
     a.in_dtype = p->dtype_input;
+    a.split_k = p->split_k_slices > 1 ? p->split_k_slices : 0;
     e = scb::launch_conv_wgrad(a, sms, s);
     if (e != cudaSuccess) return cuda_fail(e, "conv wgrad launch");
     scb::EpiParams ep{};

@@ -638,7 +638,8 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t 
   per_group = (P.n_mtiles + n_groups - 1) / n_groups;
   P.tiles_per_group = per_group;
   P.n_groups = (P.n_mtiles + per_group - 1) / per_group;
-  int splits = (num_sms + P.n_groups - 1) / P.n_groups;
+  // row splits: the caller's split_k_slices, else about one CTA per SM
+  int splits = a.split_k > 0 ? a.split_k : (num_sms + P.n_groups - 1) / P.n_groups;
   if (splits > P.n_chunks) splits = P.n_chunks;
   P.chunks_per_cta = (P.n_chunks + splits - 1) / splits;
   splits = (P.n_chunks + P.chunks_per_cta - 1) / P.chunks_per_cta;

@@ -87,6 +87,7 @@ struct ConvWgradArgs {
   // is b_inds ? b_inds[r] : r; dOut row is argsort ? argsort[r] : r; mask may be null
   const int32_t *b_inds;
   const int32_t *idx_sorted; // optional [kv, N]: indices[k][argsort[r]]
+  int split_k;               // row splits (grid.x); 0 = about one CTA per SM
 };
 cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t stream);
 
