@@ -42,8 +42,6 @@
 namespace scb {
 namespace {
 
-constexpr int kThreads = 544;
-constexpr int kIdxStages = 3;
 constexpr int kTileM = 128;
 
 struct Meta {
@@ -163,15 +161,35 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
 
 // ------------------------------------------------------------------ kernel
 // Warp roles (17 warps):
-constexpr int kEpiWarps = 4;     // warps 0-3
-constexpr int kProdWarp0 = 4;    // warps 4-11
-constexpr int kProdWarps = 8;
-constexpr int kLoadWarp0 = 12;   // warps 12-15
-constexpr int kMmaWarp = 16;
+// Two layouts.  Single (one CTA per SM, 17 warps): warps 0-3 epilogue, 4-11
+// producers, 12-15 index loaders, 16 MMA; 3-deep index ring.  Pair (two
+// CTAs per SM, 11 warps each, for the gather path when two fit): warps 0-3
+// epilogue, 4-7 producers, 8-9 index loaders (2 rows per thread), 10 MMA;
+// 2-deep index ring.  Measured on B200: two CTAs per SM gather ~1.5x the
+// rows per cycle of one (the TMA gather rate is per issuing CTA, not per SM).
+constexpr int kEpiWarps = 4;  // warps 0-3 in both layouts
+constexpr int kProdWarp0 = 4;
+template <bool kPair> struct Layout {
+  static constexpr int kProdWarps = kPair ? 4 : 8;
+  static constexpr int kLoadWarp0 = kProdWarp0 + kProdWarps;
+  static constexpr int kLoadWarps = kPair ? 2 : 4;
+  static constexpr int kMmaWarp = kLoadWarp0 + kLoadWarps;
+  static constexpr int kThreads = (kMmaWarp + 1) * 32;
+  static constexpr int kIdxStages = kPair ? 2 : 3;
+  static constexpr int kRowsPer = kTileM / (kLoadWarps * 32);
+};
 
-template <bool kF8, typename TOut, bool kTma, bool kGather>
-__global__ void __maxnreg__(96)
+// Registers: single layout 17 warps (5 per SMSP) x 96; pair layout 2 x 11
+// warps (up to 6 per SMSP) x 80 = 15360 of an SMSP's 16K registers.
+template <bool kF8, typename TOut, bool kTma, bool kGather, bool kPair>
+__global__ void __maxnreg__(kPair ? 80 : 96)
     conv_rowgather_kernel(const __grid_constant__ KParams P) {
+  constexpr int kProdWarps = Layout<kPair>::kProdWarps;
+  constexpr int kLoadWarp0 = Layout<kPair>::kLoadWarp0;
+  constexpr int kLoadWarps = Layout<kPair>::kLoadWarps;
+  constexpr int kMmaWarp = Layout<kPair>::kMmaWarp;
+  constexpr int kIdxStages = Layout<kPair>::kIdxStages;
+  constexpr int kRowsPer = Layout<kPair>::kRowsPer;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_u32 = smem_u32(smem_raw);
   const uint32_t pad = (1024u - (raw_u32 & 1023u)) & 1023u;
@@ -207,7 +225,7 @@ __global__ void __maxnreg__(96)
       mbar_init(&empty_bar[i], 1);
     }
     for (int i = 0; i < kIdxStages; ++i) {
-      mbar_init(&idx_full[i], 128);
+      mbar_init(&idx_full[i], kLoadWarps * 32);
       mbar_init(&idx_empty[i], (kGather ? kProdWarps : min(S, kProdWarps)) + 1);
     }
     for (int i = 0; i < 2; ++i) {
@@ -230,10 +248,11 @@ __global__ void __maxnreg__(96)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  if (warp >= kLoadWarp0 && warp < kLoadWarp0 + 4) {
+  if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
     // ---------------------------------------------------------------- index loaders
-    const int r = threadIdx.x - kLoadWarp0 * 32;  // row inside the tile
-    const int lw = r >> 5;
+    // kLoadWarps warps, kRowsPer rows of the tile per thread (row t + i * 32 kLoadWarps)
+    const int t = threadIdx.x - kLoadWarp0 * 32;
+    const int lw = t >> 5;
     for (int it = 0;; ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
@@ -272,91 +291,100 @@ __global__ void __maxnreg__(96)
         tile = sched_tile[it & 3];
       }
       if (tile < 0) {
-        if (r == 0) meta->tile = -1;
+        if (t == 0) meta->tile = -1;
         mbar_arrive(&idx_full[b]);
         break;
       }
       const int64_t tile_m = tile / A.n_tiles;
       const int n_tile = static_cast<int>(tile % A.n_tiles);
-      const int64_t row_g = tile_m * kTileM + r;
-      const bool valid = row_g < A.M;
-      // Every index of the row (all kv offsets) is loaded up front and stored
-      // unconditionally below, so the loads leave together: one memory round
-      // trip per tile.  With the sorted table row_g is already the sorted row;
-      // otherwise sigma(row) comes first (argsort), then the kv loads.
-      int pre[32];
-      if (A.idx_sorted) {
+      uint32_t g0 = 0, g1 = 0, g2 = 0, g3 = 0, tm = 0;
+#pragma unroll 1
+      for (int rr = 0; rr < kRowsPer; ++rr) {
+        const int r = t + rr * (kLoadWarps * 32);  // row inside the tile
+        const int64_t row_g = tile_m * kTileM + r;
+        const bool valid = row_g < A.M;
+        // Every index of the row (all kv offsets) is loaded up front and stored
+        // unconditionally below, so the loads leave together: one memory round
+        // trip per row.  With the sorted table row_g is already the sorted row;
+        // otherwise sigma(row) comes first (argsort), then the kv loads.
+        int pre[32];
+        if (A.idx_sorted) {
 #pragma unroll
-        for (int k = 0; k < 32; ++k)
-          pre[k] = (valid && k < A.kv) ? __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.M + row_g)
-                                       : -1;
-      } else {
-        int sig = valid ? (A.argsort ? __ldg(A.argsort + row_g) : static_cast<int>(row_g)) : -1;
-        if (valid && (sig < 0 || sig >= A.out_rows)) {
-          flag_error(A.err, kErrBadIndex);
-          sig = -1;
-        }
-        int ident = -1;
-        if (!A.indices && sig >= 0) ident = A.a_inds ? __ldg(A.a_inds + row_g) : static_cast<int>(row_g);
-#pragma unroll
-        for (int k = 0; k < 32; ++k)
-          pre[k] = (sig >= 0 && k < A.kv)
-                       ? (A.indices ? __ldg(A.indices + static_cast<int64_t>(k) * A.M + sig) : ident)
-                       : -1;
-      }
-      // every loader warp reduces all four 32-row groups itself (no cross-warp
-      // barrier, so an aborted warp can never strand the others)
-      uint32_t gq[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int64_t rr = tile_m * kTileM + q * 32 + lane;
-        uint32_t v = rr < A.M ? (A.mask ? __ldg(A.mask + rr) : 1u) : 0u;
-#pragma unroll
-        for (int s = 16; s > 0; s >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, s);
-        gq[q] = v;
-      }
-      const uint32_t g0 = gq[0], g1 = gq[1], g2 = gq[2], g3 = gq[3];
-      uint32_t tm = (g0 | g1 | g2 | g3) & A.mask_filter;
-      uint32_t sub;
-      if (A.tile_m_desp == 32) {
-        sub = lw == 0 ? g0 : lw == 1 ? g1 : lw == 2 ? g2 : g3;
-      } else if (A.tile_m_desp == 64) {
-        sub = lw < 2 ? (g0 | g1) : (g2 | g3);
-      } else {
-        sub = g0 | g1 | g2 | g3;
-      }
-      sub &= A.mask_filter;
-      if (A.is_fwd && A.mask_out != nullptr && n_tile == 0 && r == 0) {
-        const int nsub = kTileM / A.tile_m_desp;
-        for (int d = 0; d < nsub; ++d) {
-          const int64_t start = tile_m * kTileM + d * A.tile_m_desp;
-          if (start >= A.M) break;
-          uint32_t w;
-          if (nsub == 4) w = d == 0 ? g0 : d == 1 ? g1 : d == 2 ? g2 : g3;
-          else if (nsub == 2) w = d == 0 ? (g0 | g1) : (g2 | g3);
-          else w = g0 | g1 | g2 | g3;
-          A.mask_out[start / A.tile_m_desp] = w & A.mask_filter;
-        }
-      }
-      if (A.reverse) {
-        tm = __brev(tm) >> (32 - A.kv);
-        sub = __brev(sub) >> (32 - A.kv);
-      }
-      // tab[k][r]: index of row r for offset k (-1 where the row's sub-tile
-      // mask lacks k).  Written for every offset, whatever the tile mask: a
-      // select, not a branch, so no load is deferred to its use.
-#pragma unroll
-      for (int k = 0; k < 32; ++k) {
-        if (k < A.kv) {
-          int v = ((sub >> k) & 1u) ? pre[k] : -1;
-          if (v < -1 || v >= A.a_rows) {
+          for (int k = 0; k < 32; ++k)
+            pre[k] = (valid && k < A.kv) ? __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.M + row_g)
+                                         : -1;
+        } else {
+          int sig = valid ? (A.argsort ? __ldg(A.argsort + row_g) : static_cast<int>(row_g)) : -1;
+          if (valid && (sig < 0 || sig >= A.out_rows)) {
             flag_error(A.err, kErrBadIndex);
-            v = -1;
+            sig = -1;
           }
-          tab[k * kTileM + r] = v;
+          int ident = -1;
+          if (!A.indices && sig >= 0) ident = A.a_inds ? __ldg(A.a_inds + row_g) : static_cast<int>(row_g);
+#pragma unroll
+          for (int k = 0; k < 32; ++k)
+            pre[k] = (sig >= 0 && k < A.kv)
+                         ? (A.indices ? __ldg(A.indices + static_cast<int64_t>(k) * A.M + sig) : ident)
+                         : -1;
+        }
+        if (rr == 0) {
+          // every loader warp reduces all four 32-row groups itself (no
+          // cross-warp barrier, so an aborted warp can never strand the others)
+          uint32_t gq[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int64_t rq = tile_m * kTileM + q * 32 + lane;
+            uint32_t v = rq < A.M ? (A.mask ? __ldg(A.mask + rq) : 1u) : 0u;
+#pragma unroll
+            for (int sh = 16; sh > 0; sh >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, sh);
+            gq[q] = v;
+          }
+          g0 = gq[0];
+          g1 = gq[1];
+          g2 = gq[2];
+          g3 = gq[3];
+          tm = (g0 | g1 | g2 | g3) & A.mask_filter;
+          if (A.is_fwd && A.mask_out != nullptr && n_tile == 0 && t == 0) {
+            const int nsub = kTileM / A.tile_m_desp;
+            for (int d = 0; d < nsub; ++d) {
+              const int64_t start = tile_m * kTileM + d * A.tile_m_desp;
+              if (start >= A.M) break;
+              uint32_t w;
+              if (nsub == 4) w = d == 0 ? g0 : d == 1 ? g1 : d == 2 ? g2 : g3;
+              else if (nsub == 2) w = d == 0 ? (g0 | g1) : (g2 | g3);
+              else w = g0 | g1 | g2 | g3;
+              A.mask_out[start / A.tile_m_desp] = w & A.mask_filter;
+            }
+          }
+          if (A.reverse) tm = __brev(tm) >> (32 - A.kv);
+        }
+        const int lr = r >> 5;  // 32-row group of this row
+        uint32_t sub;
+        if (A.tile_m_desp == 32) {
+          sub = lr == 0 ? g0 : lr == 1 ? g1 : lr == 2 ? g2 : g3;
+        } else if (A.tile_m_desp == 64) {
+          sub = lr < 2 ? (g0 | g1) : (g2 | g3);
+        } else {
+          sub = g0 | g1 | g2 | g3;
+        }
+        sub &= A.mask_filter;
+        if (A.reverse) sub = __brev(sub) >> (32 - A.kv);
+        // tab[k][r]: index of row r for offset k (-1 where the row's sub-tile
+        // mask lacks k).  Written for every offset, whatever the tile mask: a
+        // select, not a branch, so no load is deferred to its use.
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          if (k < A.kv) {
+            int v = ((sub >> k) & 1u) ? pre[k] : -1;
+            if (v < -1 || v >= A.a_rows) {
+              flag_error(A.err, kErrBadIndex);
+              v = -1;
+            }
+            tab[k * kTileM + r] = v;
+          }
         }
       }
-      if (r == 0) {
+      if (t == 0) {
         const int na = __popc(tm);
         int s = 0;
         uint32_t mm = tm;
@@ -711,15 +739,17 @@ __global__ void __maxnreg__(96)
 }
 
 template <bool kF8, typename TOut>
-cudaError_t launch_typed(const KParams &P, bool tma, bool gather, int grid, size_t smem,
+cudaError_t launch_typed(const KParams &P, bool tma, bool gather, bool pair, int grid, size_t smem,
                          cudaStream_t stream) {
-  void (*kern)(KParams) = gather ? conv_rowgather_kernel<kF8, TOut, true, true>
-                          : tma  ? conv_rowgather_kernel<kF8, TOut, true, false>
-                                 : conv_rowgather_kernel<kF8, TOut, false, false>;
+  void (*kern)(KParams) =
+      gather ? (pair ? conv_rowgather_kernel<kF8, TOut, true, true, true>
+                     : conv_rowgather_kernel<kF8, TOut, true, true, false>)
+      : tma  ? conv_rowgather_kernel<kF8, TOut, true, false, false>
+             : conv_rowgather_kernel<kF8, TOut, false, false, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  kern<<<grid, kThreads, smem, stream>>>(P);
+  kern<<<grid, pair ? Layout<true>::kThreads : Layout<false>::kThreads, smem, stream>>>(P);
   return cudaGetLastError();
 }
 
@@ -757,26 +787,6 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
     P.opc = 128 / a.a_row_bytes;
     P.upo = a.a_row_bytes / 16;
   }
-  const uint32_t a_bytes = kTileM * static_cast<uint32_t>(P.row_bytes);
-  const uint32_t b_bytes = static_cast<uint32_t>(a.BN) * P.row_bytes;
-  P.stage_bytes = a_bytes + b_bytes;
-  P.b_off = a_bytes;
-  P.idx_buf_bytes = ((static_cast<uint32_t>(a.kv) * kTileM * 4 + sizeof(Meta)) + 127u) & ~127u;
-  const uint32_t idx_total = P.idx_buf_bytes * kIdxStages;
-  const uint32_t bar_bytes = 512;
-  const uint32_t budget = 227u * 1024u - 1024u - idx_total - bar_bytes;
-  int stages = static_cast<int>(budget / P.stage_bytes);
-  if (stages > 8) stages = 8;
-  if (stages < 2) return cudaErrorInvalidConfiguration;
-  P.stages = stages;
-  P.idx_off = P.stage_bytes * stages;
-  P.bar_off = P.idx_off + idx_total;
-  const size_t smem = 1024 + P.bar_off + bar_bytes;
-  uint32_t cols = 32;
-  while (cols < static_cast<uint32_t>(2 * a.BN)) cols <<= 1;
-  P.tmem_cols = cols;
-  if (P.num_tiles == 0) return cudaSuccess;
-  const int grid = static_cast<int>(P.num_tiles < num_sms ? P.num_tiles : num_sms);
   // TMA weight slabs: whole 128-byte reduction chunks (no packing of small offsets)
   if (P.cpo > 0 && P.row_bytes == 128) {
     const uint32_t box = 128u / esz;
@@ -787,19 +797,49 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
       gather = encode_tmap_2d(&P.tmap_a, a.in_dtype, a.a_base, red, static_cast<uint64_t>(a.a_rows),
                               static_cast<uint64_t>(a.a_row_stride), box, 1);
   }
+  const uint32_t a_bytes = kTileM * static_cast<uint32_t>(P.row_bytes);
+  const uint32_t b_bytes = static_cast<uint32_t>(a.BN) * P.row_bytes;
+  P.stage_bytes = a_bytes + b_bytes;
+  P.b_off = a_bytes;
+  P.idx_buf_bytes = ((static_cast<uint32_t>(a.kv) * kTileM * 4 + sizeof(Meta)) + 127u) & ~127u;
+  uint32_t cols = 32;
+  while (cols < static_cast<uint32_t>(2 * a.BN)) cols <<= 1;
+  P.tmem_cols = cols;
+  const uint32_t bar_bytes = 512;
+  // dynamic shared memory of one CTA: 227 KB alone on an SM, 113 KB for two
+  // per SM; 1 KB of it is slack for the 1024-byte alignment of the stages
+  auto stages_for = [&](uint32_t limit, int idx_stages) {
+    const int64_t budget = static_cast<int64_t>(limit) - 1024 - P.idx_buf_bytes * idx_stages - bar_bytes;
+    const int64_t st = budget / P.stage_bytes;
+    return static_cast<int>(st > 8 ? 8 : st);
+  };
+  const uint32_t kLimitSingle = 227u * 1024u, kLimitPair = 113u * 1024u;
+  // two CTAs per SM on the gather path when both fit (TMEM: 2 x 2 BN columns)
+  // with at least 3 stages each
+  const bool pair = gather && cols <= 256 && stages_for(kLimitPair, Layout<true>::kIdxStages) >= 3;
+  const int idx_stages = pair ? Layout<true>::kIdxStages : Layout<false>::kIdxStages;
+  const int stages = stages_for(pair ? kLimitPair : kLimitSingle, idx_stages);
+  if (stages < 2) return cudaErrorInvalidConfiguration;
+  P.stages = stages;
+  P.idx_off = P.stage_bytes * stages;
+  P.bar_off = P.idx_off + P.idx_buf_bytes * idx_stages;
+  const size_t smem = 1024 + P.bar_off + bar_bytes;
+  if (P.num_tiles == 0) return cudaSuccess;
+  const int64_t ctas = static_cast<int64_t>(pair ? 2 : 1) * num_sms;
+  const int grid = static_cast<int>(P.num_tiles < ctas ? P.num_tiles : ctas);
   if (a.in_dtype == 14) {
     P.idesc = make_idesc(128, a.BN, 0u, false, false);
     switch (a.out_dtype) {
-      case 0: return launch_typed<true, float>(P, tma, gather, grid, smem, stream);
-      case 7: return launch_typed<true, __half>(P, tma, gather, grid, smem, stream);
-      default: return launch_typed<true, __nv_bfloat16>(P, tma, gather, grid, smem, stream);
+      case 0: return launch_typed<true, float>(P, tma, gather, pair, grid, smem, stream);
+      case 7: return launch_typed<true, __half>(P, tma, gather, pair, grid, smem, stream);
+      default: return launch_typed<true, __nv_bfloat16>(P, tma, gather, pair, grid, smem, stream);
     }
   }
   P.idesc = make_idesc(128, a.BN, a.in_dtype == 12 ? 1u : 0u, false, false);
   switch (a.out_dtype) {
-    case 0: return launch_typed<false, float>(P, tma, gather, grid, smem, stream);
-    case 7: return launch_typed<false, __half>(P, tma, gather, grid, smem, stream);
-    case 12: return launch_typed<false, __nv_bfloat16>(P, tma, gather, grid, smem, stream);
+    case 0: return launch_typed<false, float>(P, tma, gather, pair, grid, smem, stream);
+    case 7: return launch_typed<false, __half>(P, tma, gather, pair, grid, smem, stream);
+    case 12: return launch_typed<false, __nv_bfloat16>(P, tma, gather, pair, grid, smem, stream);
     default: break;
   }
   return cudaErrorInvalidValue;
