@@ -17,22 +17,25 @@
 // sub-tile (32/64/128) gates its own rows, which keeps results identical to a
 // tile_shape[0]-row kernel even for masks inconsistent with the index table.
 //
-// B200 design (one persistent CTA per SM, 17 warps, warp-specialised):
-//   warps 0-3   epilogue: TMEM -> registers -> permuted row stores
-//   warps 4-11  producers: 16-byte cp.async gathers of the A rows that have a
-//               pair into SWIZZLE_128B shared-memory stages (one 128-byte
-//               reduction chunk per stage, 16 rows per warp, all warps on
-//               every stage); rows without a pair are
-//               zero-filled copies (no memory request; a shared store would
-//               need a proxy fence that waits on the thread's copies in
-//               flight); the weight slab arrives by one 2-D TMA load.
-//               Measured on B200: scattered 128-byte rows reach ~100 GB/s per
-//               SM through cp.async from 8+ warps, TMA tile::gather4 only
-//               ~13 GB/s per issuing warp, so the gather stays on cp.async.
-//   warps 12-15 index loaders: mask / argsort / indices of the next tiles into
-//               a 3-deep shared-memory ring (hides the argsort->index latency)
-//   warp 16     TMEM allocator + single-thread tcgen05.mma issuer into a
-//               double-buffered fp32 TMEM accumulator (128 lanes x BN columns)
+// B200 design (persistent, warp-specialised; tiles drawn from a per-call
+// counter so CTAs that drew small tiles come back for more):
+//   epilogue warps   TMEM -> registers -> act(alpha acc + beta src) -> row
+//                    mask_argsort[r] (permuted store)
+//   producer warps   A rows of each (offset, 128-byte column block) chunk by
+//                    TMA tile::gather4 (4 rows per lane, SWIZZLE_128B or
+//                    SWIZZLE_64B by address; index -1 reads as zero rows) and
+//                    the weight slab by one 2-D TMA box; shorter rows (16 / 32
+//                    bytes, several offsets packed per 128-byte row) by 16-byte
+//                    cp.async instead
+//   loader warps     tile masks (OR, mask_filter, brev for backward-input),
+//                    mask_output, and the tile's [offset][row] index table into
+//                    a shared-memory ring, all loads of a row issued together
+//   MMA warp         TMEM allocator + single-thread tcgen05.mma issuer into a
+//                    double-buffered fp32 TMEM accumulator (128 lanes x BN)
+// Layouts (Layout<kPair>): one 17-warp CTA per SM, or on the gather path two
+// 11-warp CTAs per SM (4 producers, 2 loaders): measured on B200 the TMA
+// gather rate is per issuing CTA, so two CTAs per SM gather ~1.5x the rows
+// per cycle, which the kernel, bound by that rate, turns into ~12 % less time.
 // Every mbarrier wait is bounded (globaltimer) and raises a CTA abort flag
 // plus kErrWaitTimeout instead of spinning forever.
 #include <cuda.h>
