@@ -15,11 +15,13 @@
 // matching 64 dOut rows are the N side.  Every CTA owns a group of M-tiles
 // (up to 512 TMEM columns of fp32 accumulators) and every splits-th row
 // chunk; TMEM accumulates over the whole range, and the epilogue adds the
-// CTA's partial dW into an fp32 workspace with red.global.add (split over rows
-// without a serial semaphore, so there is no inter-CTA spin).  A finalize
-// kernel applies alpha/beta and converts to the weight dtype.
-// Warp roles are the same as the forward kernel: 0-3 epilogue, 4-11 cp.async
-// producers, 12-15 index loaders, 16 TMEM allocator + tcgen05.mma issuer.
+// CTA's partial dW into an fp32 workspace with red.global.add.v4.f32 (split
+// over rows without a serial semaphore, so there is no inter-CTA spin).  A
+// finalize kernel applies alpha/beta and converts to the weight dtype.
+// Warp roles (one 17-warp CTA per SM): 0-3 epilogue, 4-11 producers (TMA
+// tile::gather4 of the input rows per stage and of the chunk's dOut rows once
+// per chunk when rows are whole 128-byte blocks, 16-byte cp.async otherwise),
+// 12-15 index loaders, 16 TMEM allocator + tcgen05.mma issuer.
 #include <cuda.h>
 
 #include "kernels.h"
