@@ -29,13 +29,15 @@
 namespace scb {
 namespace {
 
+// 17 warps (5 per SM sub-partition at 96 registers)
 constexpr int kThreads = 544;
 constexpr int kEpiWarps = 4;     // warps 0-3
 constexpr int kProdWarp0 = 4;    // warps 4-11
 constexpr int kProdWarps = 8;
 constexpr int kLoadWarp0 = 12;   // warps 12-15
 constexpr int kMmaWarp = 16;
-constexpr int kIdxStages = 3;
+constexpr int kIdxStages = 4;
+constexpr int kMaxBBufs = 4;  // dOut buffers of the gather path (2 or 4 per launch)
 constexpr int kRows = 64;  // reduction rows per stage
 
 struct WMeta {
@@ -58,10 +60,12 @@ struct WParams {
   int fpa;             // filters per atom (C < 64)
   int upf;             // 16-byte units per filter segment (C < 64)
   int n_mma;           // MMA N (K rounded up to 64)
+  int mw_shift;        // log2(mask_width) when it is a power of two, else -1
   int stages;
   uint32_t stage_bytes;
   uint32_t b_off;
-  uint32_t bbuf_off;      // gather path: two dOut buffers of n_b_atoms x 8 KB
+  uint32_t bbuf_off;      // gather path: n_bbuf dOut buffers of n_b_atoms x 8 KB
+  uint32_t n_bbuf;
   uint32_t idx_off;
   uint32_t idx_buf_bytes;
   uint32_t bar_off;
@@ -139,10 +143,11 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
   uint64_t *acc_full = idx_empty + kIdxStages;
   uint64_t *drain_bar = acc_full + 1;
   uint64_t *bfull = drain_bar + 1;   // gather path: dOut buffer b loaded
-  uint64_t *bempty = bfull + 2;      // gather path: dOut buffer b consumed
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bempty + 2);
+  uint64_t *bempty = bfull + kMaxBBufs;  // gather path: dOut buffer b consumed
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bempty + kMaxBBufs);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
   uint32_t *used_tiles = reinterpret_cast<uint32_t *>(tmem_slot + 2);
+  uint32_t *tile_fbits = used_tiles + 1;  // [16]: filters of M-tile t0 + j
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -168,12 +173,13 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
     }
     mbar_init(acc_full, 1);
     mbar_init(drain_bar, 1);
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kMaxBBufs; ++i) {
       mbar_init(&bfull[i], kProdWarps);
       mbar_init(&bempty[i], 1);
     }
     *abort_flag = 0;
     *used_tiles = 0;
+    for (int j = 0; j < 16; ++j) tile_fbits[j] = t0 + j < t1 ? tile_filter_bits(P, t0 + j) : 0u;
     fence_mbar_init();
   }
   if (warp == kMmaWarp) {
@@ -203,62 +209,60 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       int *sig_tab = tab + 32 * kRows;                   // [64]
       WMeta *meta = reinterpret_cast<WMeta *>(sig_tab + kRows);
       const int64_t row = static_cast<int64_t>(c) * kRows + r;
+      const int64_t row2 = static_cast<int64_t>(c) * kRows + (r ^ 32);
       const bool valid = row < A.N;
+      // Every load of the chunk leaves before any result is used (argsort,
+      // the mask words of this row and of its partner row r ^ 32, and with
+      // the sorted table the indices): one memory round trip per chunk.
       int sig = valid ? (A.argsort ? __ldg(A.argsort + row) : static_cast<int>(row)) : -1;
-      if (valid && (sig < 0 || sig >= A.dout_rows)) {
-        flag_error(A.err, kErrBadIndex);
-        sig = -1;
-      }
-      uint32_t word = 0;
-      if (valid) {
-        if (A.mask) {
-          const int64_t wi = row / A.mask_width;
+      uint32_t word = 0, w_other = 0;
+      if (A.mask) {
+        if (valid) {
+          const int64_t wi = P.mw_shift >= 0 ? row >> P.mw_shift : row / A.mask_width;
           if (wi < A.mask_count) word = __ldg(A.mask + wi);
-        } else {
-          word = 0xffffffffu;
         }
-      }
-      word &= A.mask_filter;
-      // this warp covers rows (r & 32) .. +31; the partner half of the chunk is
-      // the same rows one warp over, so OR the words of both 32-row halves
-      // without a cross-warp barrier (rows r and r ^ 32 share a mask word
-      // unless mask_width < 64; read both explicitly)
-      uint32_t w_other = 0;
-      {
-        const int64_t row2 = static_cast<int64_t>(c) * kRows + (r ^ 32);
         if (row2 < A.N) {
-          if (A.mask) {
-            const int64_t wi = row2 / A.mask_width;
-            if (wi < A.mask_count) w_other = __ldg(A.mask + wi);
-          } else {
-            w_other = 0xffffffffu;
-          }
+          const int64_t wi = P.mw_shift >= 0 ? row2 >> P.mw_shift : row2 / A.mask_width;
+          if (wi < A.mask_count) w_other = __ldg(A.mask + wi);
         }
-        w_other &= A.mask_filter;
+      } else {
+        word = valid ? 0xffffffffu : 0u;
+        w_other = row2 < A.N ? 0xffffffffu : 0u;
       }
-      uint32_t gw = word | w_other;
-#pragma unroll
-      for (int s = 16; s > 0; s >>= 1) gw |= __shfl_xor_sync(0xffffffffu, gw, s);
-      if (half == 0) sig_tab[r] = sig;
-      const uint32_t cm = gw;
-      // every index of the thread's filters is loaded up front and gated by a
-      // select afterwards, so the loads leave together (one round trip)
       int vals[16];
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
         const int k = k_lo + 2 * q + half;
-        int v = -1;
-        if (k < k_hi) {
-          if (A.idx_sorted) {  // coalesced: row is the sorted row
-            if (valid) v = __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.N + row);
-          } else if (A.indices) {
-            if (sig >= 0) v = __ldg(A.indices + static_cast<int64_t>(k) * A.N + sig);
-          } else if (sig >= 0) {
-            v = A.b_inds ? __ldg(A.b_inds + row) : static_cast<int>(row);
-          }
-        }
-        vals[q] = v;
+        vals[q] = (A.idx_sorted && valid && k < k_hi)  // coalesced: row is the sorted row
+                      ? __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.N + row)
+                      : -1;
       }
+      if (valid && (sig < 0 || sig >= A.dout_rows)) {
+        flag_error(A.err, kErrBadIndex);
+        sig = -1;
+      }
+      if (!A.idx_sorted) {  // indices of the unsorted table are read at row sigma(r)
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int k = k_lo + 2 * q + half;
+          int v = -1;
+          if (k < k_hi && sig >= 0) {
+            if (A.indices) v = __ldg(A.indices + static_cast<int64_t>(k) * A.N + sig);
+            else v = A.b_inds ? __ldg(A.b_inds + row) : static_cast<int>(row);
+          }
+          vals[q] = v;
+        }
+      }
+      word &= A.mask_filter;
+      w_other &= A.mask_filter;
+      // this warp covers rows (r & 32) .. +31 and read the words of the
+      // partner rows r ^ 32 too (rows r and r ^ 32 share a mask word unless
+      // mask_width < 64), so the OR over the warp is the chunk's mask, with
+      // no cross-warp barrier
+      uint32_t cm = word | w_other;
+#pragma unroll
+      for (int s = 16; s > 0; s >>= 1) cm |= __shfl_xor_sync(0xffffffffu, cm, s);
+      if (half == 0) sig_tab[r] = sig;
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
         const int k = k_lo + 2 * q + half;
@@ -271,15 +275,15 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
           tab[(k - k_lo) * kRows + r] = v;
         }
       }
-      if (t == 0) {
-        uint32_t bits = 0;
-        for (int tt = t0; tt < t1; ++tt)
-          if (tile_filter_bits(P, tt) & cm) bits |= 1u << (tt - t0);
-        meta->active_bits = bits;
-        meta->n_active = __popc(bits);
+      if (t < 32) {
+        // lane j tests M-tile t0 + j against the chunk mask
+        const bool on = lane < t1 - t0 && (tile_fbits[lane] & cm) != 0;
+        const uint32_t bits = __ballot_sync(0xffffffffu, on);
+        if (t == 0) {
+          meta->active_bits = bits;
+          meta->n_active = __popc(bits);
+        }
       }
-      // grp[] of this buffer is rewritten only after idx_empty, i.e. after all
-      // loader threads passed the named barrier of this chunk
       mbar_arrive(&idx_full[b]);
     }
   } else if (warp >= kProdWarp0 && warp < kProdWarp0 + kProdWarps) {
@@ -293,17 +297,21 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
     // cp.async (src-size 0, no memory request).
     const int pw = warp - kProdWarp0;
     if constexpr (kGather) {
-    // TMA gather: all kProdWarps warps serve every stage.  Lane l < 4 of warp
-    // pw issues one tile::gather4 for rows 8 pw + 4 (l & 1) .. +3 of atom
-    // l >> 1 (input rows of the atom's filter; index -1 lands as zeros).
+    // TMA gather: all kProdWarps warps serve every stage.  Warp pw owns rows
+    // [kRpw pw, kRpw pw + kRpw) of each 64-row atom; lane l < 2 kGpw issues
+    // one tile::gather4 for rows kRpw pw + 4 (l % kGpw) .. +3 of atom
+    // l / kGpw (input rows of the atom's filter; index -1 lands as zeros).
     // The chunk's 64 dOut rows are the same for every M-tile, so they are
-    // gathered once per chunk into one of two dOut buffers (lanes
-    // l < 2 n_b_atoms, same row split), released by the MMA after the chunk's
-    // last tile.  Lane 0 of each warp arrives with expect_tx for its bytes.
+    // gathered once per chunk into one of n_bbuf dOut buffers (lanes
+    // l < kGpw n_b_atoms, same row split), released by the MMA after the
+    // chunk's last tile.  Lane 0 of each warp arrives with expect_tx for its
+    // bytes.
+    constexpr int kRpw = kRows / kProdWarps;  // 8 rows per warp
+    constexpr int kGpw = kRpw / 4;            // 2 gathers per atom per warp
     const int n_b_atoms = P.n_mma / 64;
-    const int rq = pw * 8 + (lane & 1) * 4;
+    const int rq = pw * kRpw + (lane % kGpw) * 4;
     int it = 0;
-    uint32_t stage = 0, eph = 0, ub = 0;
+    uint32_t stage = 0, eph = 0, bb = 0, bph = 0;  // dOut buffer and its phase
     bool ok = true;
     for (int c = c_begin; c < c_end && ok; c += c_step, ++it) {
       const int b = it % kIdxStages;
@@ -318,20 +326,22 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       const WMeta *meta = reinterpret_cast<const WMeta *>(sig_tab + kRows);
       uint32_t bits = meta->active_bits;
       if (bits) {
-        const uint32_t bb = ub & 1u;
-        if (!__all_sync(0xffffffffu, mbar_wait(&bempty[bb], ((ub >> 1) & 1u) ^ 1u, abort_flag))) {
+        if (!__all_sync(0xffffffffu, mbar_wait(&bempty[bb], bph ^ 1u, abort_flag))) {
           if (lane == 0) flag_error(A.err, kErrWaitTimeout);
           break;
         }
-        if (lane == 0) mbar_arrive_expect_tx(&bfull[bb], static_cast<uint32_t>(n_b_atoms) * 1024u);
+        if (lane == 0) mbar_arrive_expect_tx(&bfull[bb], static_cast<uint32_t>(n_b_atoms * kRpw) * 128u);
         __syncwarp();
-        if (lane < 2 * n_b_atoms) {
-          const int na = lane >> 1;
+        if (lane < kGpw * n_b_atoms) {
+          const int na = lane / kGpw;
           const int4 q = *reinterpret_cast<const int4 *>(sig_tab + rq);
           tma_gather4(smem_base + P.bbuf_off + bb * (n_b_atoms * 8192u) + na * 8192u + rq * 128,
                       &P.tmap_dout, na * 64, q.x, q.y, q.z, q.w, &bfull[bb]);
         }
-        ++ub;
+        if (++bb == P.n_bbuf) {
+          bb = 0;
+          bph ^= 1u;
+        }
       }
       while (bits) {
         const int jt = __ffs(bits) - 1;
@@ -347,15 +357,15 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
           stage = 0;
           eph ^= 1u;
         }
-        if (lane == 0) mbar_arrive_expect_tx(&full_bar[s], 2048u);
+        if (lane == 0) mbar_arrive_expect_tx(&full_bar[s], 2u * kRpw * 128u);
         __syncwarp();
-        if (lane < 4) {
-          const int a = 2 * tt + (lane >> 1);
+        if (lane < 2 * kGpw) {
+          const int a = 2 * tt + lane / kGpw;
           const int k = a / P.cpa;
           int4 q = make_int4(-1, -1, -1, -1);
           if (a < P.n_atoms && k < A.kv)
             q = *reinterpret_cast<const int4 *>(tab + (k - k_lo) * kRows + rq);
-          tma_gather4(smem_base + s * P.stage_bytes + (lane >> 1) * 8192u + rq * 128, &P.tmap_in,
+          tma_gather4(smem_base + s * P.stage_bytes + (lane / kGpw) * 8192u + rq * 128, &P.tmap_in,
                       (a % P.cpa) * 64, q.x, q.y, q.z, q.w, &full_bar[s]);
         }
       }
@@ -459,7 +469,7 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
       int it = 0;
-      uint32_t stage = 0, fph = 0, ub = 0;
+      uint32_t stage = 0, fph = 0, bb = 0, bph = 0;
       uint32_t started = 0;
       bool ok = true;
       for (int c = c_begin; c < c_end && ok; c += c_step, ++it) {
@@ -476,11 +486,11 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
         uint32_t sBg = 0;
         const bool chunk_used = bits != 0;
         if (kGather && chunk_used) {
-          if (!mbar_wait(&bfull[ub & 1u], (ub >> 1) & 1u, abort_flag)) {
+          if (!mbar_wait(&bfull[bb], bph, abort_flag)) {
             flag_error(A.err, kErrWaitTimeout);
             break;
           }
-          sBg = smem_base + P.bbuf_off + (ub & 1u) * ((P.n_mma / 64) * 8192u);
+          sBg = smem_base + P.bbuf_off + bb * ((P.n_mma / 64) * 8192u);
         }
         while (bits) {
           const int j = __ffs(bits) - 1;
@@ -510,8 +520,11 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
           }
         }
         if (kGather && chunk_used && ok) {
-          mma_commit(&bempty[ub & 1u]);  // dOut buffer free once these MMAs finish
-          ++ub;
+          mma_commit(&bempty[bb]);  // dOut buffer free once these MMAs finish
+          if (++bb == P.n_bbuf) {
+            bb = 0;
+            bph ^= 1u;
+          }
         }
       }
       if (started) {
@@ -632,6 +645,9 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t 
   }
   P.n_mtiles = (P.n_atoms + 1) / 2;
   P.n_mma = ((a.K + 63) / 64) * 64;
+  P.mw_shift = -1;
+  for (int sh = 0; sh < 31; ++sh)
+    if (a.mask_width == (1 << sh)) P.mw_shift = sh;
   int per_group = 512 / P.n_mma;
   if (per_group > 16) per_group = 16;
   if (per_group > P.n_mtiles) per_group = P.n_mtiles;
@@ -658,13 +674,21 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t 
   const uint32_t b_bytes = static_cast<uint32_t>(P.n_mma / 64) * 8192;
   P.stage_bytes = gather ? a_bytes : a_bytes + b_bytes;
   P.b_off = a_bytes;
-  const uint32_t bbuf_bytes = gather ? 2 * b_bytes : 0;
   P.idx_buf_bytes = ((32 * kRows + kRows) * 4 + sizeof(WMeta) + 127) & ~127u;
   const uint32_t idx_total = P.idx_buf_bytes * kIdxStages;
   const uint32_t bar_bytes = 512;
-  const uint32_t budget = 227u * 1024u - 1024u - idx_total - bar_bytes - bbuf_bytes;
-  int stages = static_cast<int>(budget / P.stage_bytes);
-  if (stages > 8) stages = 8;
+  auto stages_for = [&](uint32_t bbuf_bytes) {
+    const int64_t budget = 227 * 1024 - 1024 - static_cast<int64_t>(idx_total) - bar_bytes -
+                           static_cast<int64_t>(bbuf_bytes);
+    const int64_t st = budget > 0 ? budget / P.stage_bytes : 0;
+    return static_cast<int>(st > 8 ? 8 : st);
+  };
+  // The producers can run n_bbuf - 1 chunks ahead of the MMA (a chunk's dOut
+  // buffer is released after its last M-tile): four buffers when that still
+  // leaves four stages, else two.
+  P.n_bbuf = gather ? (stages_for(kMaxBBufs * b_bytes) >= 4 ? kMaxBBufs : 2) : 1;
+  const uint32_t bbuf_bytes = gather ? P.n_bbuf * b_bytes : 0;
+  const int stages = stages_for(bbuf_bytes);
   if (stages < 2) return cudaErrorInvalidConfiguration;
   P.stages = stages;
   P.bbuf_off = P.stage_bytes * stages;
