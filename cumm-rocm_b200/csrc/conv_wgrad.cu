@@ -18,10 +18,12 @@
 // CTA's partial dW into an fp32 workspace with red.global.add.v4.f32 (split
 // over rows without a serial semaphore, so there is no inter-CTA spin).  A
 // finalize kernel applies alpha/beta and converts to the weight dtype.
-// Warp roles (one 17-warp CTA per SM): 0-3 epilogue, 4-11 producers (TMA
-// tile::gather4 of the input rows per stage and of the chunk's dOut rows once
-// per chunk when rows are whole 128-byte blocks, 16-byte cp.async otherwise),
-// 12-15 index loaders, 16 TMEM allocator + tcgen05.mma issuer.
+// Warp roles: epilogue, producers (TMA tile::gather4 of the input rows per
+// stage and of the chunk's dOut rows once per chunk when rows are whole
+// 128-byte blocks, 16-byte cp.async otherwise), index loaders, and one TMEM
+// allocator + tcgen05.mma issuer.  On the gather path with 64 dOut columns
+// two 11-warp CTAs share an SM (M-tile groups of <= 256 TMEM columns);
+// otherwise one 17-warp CTA per SM (Layout below).
 #include <cuda.h>
 
 #include "kernels.h"
@@ -29,13 +31,28 @@
 namespace scb {
 namespace {
 
-// 17 warps (5 per SM sub-partition at 96 registers)
-constexpr int kThreads = 544;
-constexpr int kEpiWarps = 4;     // warps 0-3
-constexpr int kProdWarp0 = 4;    // warps 4-11
-constexpr int kProdWarps = 8;
-constexpr int kLoadWarp0 = 12;   // warps 12-15
-constexpr int kMmaWarp = 16;
+// Two layouts.  Single (one CTA per SM, 17 warps, 96 registers): warps 0-3
+// epilogue, 4-11 producers, 12-15 index loaders (one row and one filter
+// parity per thread), 16 MMA; index tables of up to 32 filters.  Pair (two
+// CTAs per SM, 11 warps each, 80 registers; gather path with 64 dOut columns
+// and M-tile groups of <= 4 tiles = 256 TMEM columns): warps 0-3 epilogue,
+// 4-7 producers, 8-9 index loaders (one row, every filter of the group per
+// thread), 10 MMA; index tables of 8 filters.  The TMA gather rate is per
+// issuing CTA, so two CTAs on an SM gather faster than one.
+constexpr int kEpiWarps = 4;     // warps 0-3 in both layouts
+constexpr int kProdWarp0 = 4;
+template <bool kPair> struct Layout {
+  static constexpr int kProdWarps = kPair ? 4 : 8;
+  static constexpr int kLoadWarp0 = kProdWarp0 + kProdWarps;
+  static constexpr int kLoadWarps = kPair ? 2 : 4;
+  static constexpr int kMmaWarp = kLoadWarp0 + kLoadWarps;
+  static constexpr int kThreads = (kMmaWarp + 1) * 32;
+  static constexpr int kTabF = kPair ? 8 : 32;  // filters of an index table
+  // index loader thread: filters k_lo + par + kFStride q (q < kNQ), par being
+  // the thread's filter parity in the single layout
+  static constexpr int kFStride = kPair ? 1 : 2;
+  static constexpr int kNQ = kPair ? 8 : 16;
+};
 constexpr int kIdxStages = 4;
 constexpr int kMaxBBufs = 4;  // dOut buffers of the gather path (2 or 4 per launch)
 constexpr int kRows = 64;  // reduction rows per stage
@@ -125,8 +142,17 @@ __device__ __forceinline__ uint32_t tile_filter_bits(const WParams &P, int t) {
   return upto_hi & ~((1u << lo) - 1u);
 }
 
-template <bool kGather>
-__global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParams P) {
+// Registers: single 17 warps (5 per SM sub-partition) x 96; pair 2 x 11 warps
+// (6 per sub-partition) x 80 = 15360 of a sub-partition's 16384.
+template <bool kGather, bool kPair>
+__global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_constant__ WParams P) {
+  constexpr int kProdWarps = Layout<kPair>::kProdWarps;
+  constexpr int kLoadWarp0 = Layout<kPair>::kLoadWarp0;
+  constexpr int kLoadWarps = Layout<kPair>::kLoadWarps;
+  constexpr int kMmaWarp = Layout<kPair>::kMmaWarp;
+  constexpr int kTabF = Layout<kPair>::kTabF;
+  constexpr int kFStride = Layout<kPair>::kFStride;
+  constexpr int kNQ = Layout<kPair>::kNQ;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_u32 = smem_u32(smem_raw);
   const uint32_t pad = (1024u - (raw_u32 & 1023u)) & 1023u;
@@ -168,7 +194,7 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       mbar_init(&empty_bar[i], 1);
     }
     for (int i = 0; i < kIdxStages; ++i) {
-      mbar_init(&idx_full[i], 128);
+      mbar_init(&idx_full[i], kLoadWarps * 32);
       mbar_init(&idx_empty[i], (kGather ? kProdWarps : min(S, kProdWarps)) + 1);
     }
     mbar_init(acc_full, 1);
@@ -191,11 +217,11 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  if (warp >= kLoadWarp0 && warp < kLoadWarp0 + 4) {
+  if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
     // ---------------------------------------------------------------- index loaders
     const int t = threadIdx.x - kLoadWarp0 * 32;
-    const int r = t & 63;       // row of the chunk
-    const int half = t >> 6;    // filter parity handled by this thread
+    const int r = t & 63;                  // row of the chunk
+    const int par = kPair ? 0 : (t >> 6);  // filter parity of this thread (single layout)
     int it = 0;
     for (int c = c_begin; c < c_end; c += c_step, ++it) {
       const int b = it % kIdxStages;
@@ -205,8 +231,8 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
         break;
       }
       uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
-      int *tab = reinterpret_cast<int *>(buf);          // [F][64]
-      int *sig_tab = tab + 32 * kRows;                   // [64]
+      int *tab = reinterpret_cast<int *>(buf);          // [kTabF][64]
+      int *sig_tab = tab + kTabF * kRows;                // [64]
       WMeta *meta = reinterpret_cast<WMeta *>(sig_tab + kRows);
       const int64_t row = static_cast<int64_t>(c) * kRows + r;
       const int64_t row2 = static_cast<int64_t>(c) * kRows + (r ^ 32);
@@ -229,10 +255,10 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
         word = valid ? 0xffffffffu : 0u;
         w_other = row2 < A.N ? 0xffffffffu : 0u;
       }
-      int vals[16];
+      int vals[kNQ];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int k = k_lo + 2 * q + half;
+      for (int q = 0; q < kNQ; ++q) {
+        const int k = k_lo + kFStride * q + par;
         vals[q] = (A.idx_sorted && valid && k < k_hi)  // coalesced: row is the sorted row
                       ? __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.N + row)
                       : -1;
@@ -243,8 +269,8 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       }
       if (!A.idx_sorted) {  // indices of the unsorted table are read at row sigma(r)
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int k = k_lo + 2 * q + half;
+        for (int q = 0; q < kNQ; ++q) {
+          const int k = k_lo + kFStride * q + par;
           int v = -1;
           if (k < k_hi && sig >= 0) {
             if (A.indices) v = __ldg(A.indices + static_cast<int64_t>(k) * A.N + sig);
@@ -262,10 +288,10 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       uint32_t cm = word | w_other;
 #pragma unroll
       for (int s = 16; s > 0; s >>= 1) cm |= __shfl_xor_sync(0xffffffffu, cm, s);
-      if (half == 0) sig_tab[r] = sig;
+      if (par == 0) sig_tab[r] = sig;
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int k = k_lo + 2 * q + half;
+      for (int q = 0; q < kNQ; ++q) {
+        const int k = k_lo + kFStride * q + par;
         if (k < k_hi) {
           int v = (((word >> k) & 1u) && sig >= 0) ? vals[q] : -1;
           if (v < -1 || v >= A.in_rows) {
@@ -306,8 +332,8 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
     // l < kGpw n_b_atoms, same row split), released by the MMA after the
     // chunk's last tile.  Lane 0 of each warp arrives with expect_tx for its
     // bytes.
-    constexpr int kRpw = kRows / kProdWarps;  // 8 rows per warp
-    constexpr int kGpw = kRpw / 4;            // 2 gathers per atom per warp
+    constexpr int kRpw = kRows / kProdWarps;  // rows per warp: 8 single, 16 pair
+    constexpr int kGpw = kRpw / 4;            // gathers per atom per warp
     const int n_b_atoms = P.n_mma / 64;
     const int rq = pw * kRpw + (lane % kGpw) * 4;
     int it = 0;
@@ -322,7 +348,7 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       }
       const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
       const int *tab = reinterpret_cast<const int *>(buf);
-      const int *sig_tab = tab + 32 * kRows;
+      const int *sig_tab = tab + kTabF * kRows;
       const WMeta *meta = reinterpret_cast<const WMeta *>(sig_tab + kRows);
       uint32_t bits = meta->active_bits;
       if (bits) {
@@ -393,7 +419,7 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
       }
       const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
       const int *tab = reinterpret_cast<const int *>(buf);
-      const int *sig_tab = tab + 32 * kRows;
+      const int *sig_tab = tab + kTabF * kRows;
       const WMeta *meta = reinterpret_cast<const WMeta *>(sig_tab + kRows);
       uint32_t bits = meta->active_bits;
       uint32_t local = 0;  // index of the stage inside this chunk
@@ -480,7 +506,7 @@ __global__ void __maxnreg__(96) conv_wgrad_kernel(const __grid_constant__ WParam
           break;
         }
         const WMeta *meta = reinterpret_cast<const WMeta *>(smem + P.idx_off + b * P.idx_buf_bytes +
-                                                            (32 * kRows + kRows) * 4);
+                                                            (kTabF * kRows + kRows) * 4);
         uint32_t bits = meta->active_bits;
         mbar_arrive(&idx_empty[b]);
         uint32_t sBg = 0;
@@ -648,19 +674,6 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t 
   P.mw_shift = -1;
   for (int sh = 0; sh < 31; ++sh)
     if (a.mask_width == (1 << sh)) P.mw_shift = sh;
-  int per_group = 512 / P.n_mma;
-  if (per_group > 16) per_group = 16;
-  if (per_group > P.n_mtiles) per_group = P.n_mtiles;
-  // as few groups as TMEM allows, then equal shares (14 tiles: 7 + 7, not 8 + 6)
-  const int n_groups = (P.n_mtiles + per_group - 1) / per_group;
-  per_group = (P.n_mtiles + n_groups - 1) / n_groups;
-  P.tiles_per_group = per_group;
-  P.n_groups = (P.n_mtiles + per_group - 1) / per_group;
-  // row splits: the caller's split_k_slices, else about one CTA per SM
-  int splits = a.split_k > 0 ? a.split_k : (num_sms + P.n_groups - 1) / P.n_groups;
-  if (splits > P.n_chunks) splits = P.n_chunks;
-  P.chunks_per_cta = (P.n_chunks + splits - 1) / splits;
-  splits = (P.n_chunks + P.chunks_per_cta - 1) / P.chunks_per_cta;
   // gather path: whole 128-byte row blocks on both sides and tensor maps for
   // the input and dOut rows (else 16-byte cp.async gathers)
   bool gather = P.cpa > 0 && a.K % 64 == 0 && (a.in_dtype == 12 || a.in_dtype == 7) &&
@@ -674,37 +687,65 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t 
   const uint32_t b_bytes = static_cast<uint32_t>(P.n_mma / 64) * 8192;
   P.stage_bytes = gather ? a_bytes : a_bytes + b_bytes;
   P.b_off = a_bytes;
-  P.idx_buf_bytes = ((32 * kRows + kRows) * 4 + sizeof(WMeta) + 127) & ~127u;
-  const uint32_t idx_total = P.idx_buf_bytes * kIdxStages;
   const uint32_t bar_bytes = 512;
-  auto stages_for = [&](uint32_t bbuf_bytes) {
-    const int64_t budget = 227 * 1024 - 1024 - static_cast<int64_t>(idx_total) - bar_bytes -
-                           static_cast<int64_t>(bbuf_bytes);
+  auto idx_buf_for = [](bool pr) {
+    const int f = pr ? Layout<true>::kTabF : Layout<false>::kTabF;
+    return static_cast<uint32_t>(((f * kRows + kRows) * 4 + sizeof(WMeta) + 127) & ~size_t(127));
+  };
+  // stages that fit beside the index ring, barriers and dOut buffers in one
+  // CTA's dynamic shared memory: 227 KB alone on an SM, 113 KB for one of two
+  // (1 KB of it is slack for the 1024-byte alignment of the stages)
+  auto stages_for = [&](bool pr, uint32_t bbuf_bytes) {
+    const int64_t limit = pr ? 113 * 1024 : 227 * 1024;
+    const int64_t budget = limit - 1024 - static_cast<int64_t>(idx_buf_for(pr)) * kIdxStages -
+                           bar_bytes - static_cast<int64_t>(bbuf_bytes);
     const int64_t st = budget > 0 ? budget / P.stage_bytes : 0;
     return static_cast<int>(st > 8 ? 8 : st);
   };
+  // Two CTAs per SM on the gather path with 64 dOut columns, when three
+  // stages and two dOut buffers fit in 113 KB.
+  const bool pair = gather && P.n_mma == 64 && stages_for(true, 2 * b_bytes) >= 3;
   // The producers can run n_bbuf - 1 chunks ahead of the MMA (a chunk's dOut
   // buffer is released after its last M-tile): four buffers when that still
-  // leaves four stages, else two.
-  P.n_bbuf = gather ? (stages_for(kMaxBBufs * b_bytes) >= 4 ? kMaxBBufs : 2) : 1;
+  // leaves four stages (three in the pair layout), else two.
+  P.n_bbuf = gather ? (stages_for(pair, kMaxBBufs * b_bytes) >= (pair ? 3 : 4) ? kMaxBBufs : 2) : 1;
   const uint32_t bbuf_bytes = gather ? P.n_bbuf * b_bytes : 0;
-  const int stages = stages_for(bbuf_bytes);
+  const int stages = stages_for(pair, bbuf_bytes);
   if (stages < 2) return cudaErrorInvalidConfiguration;
+  P.idx_buf_bytes = idx_buf_for(pair);
+  // M-tile groups: TMEM columns per CTA (512, or 256 for each of a pair)
+  int per_group = (pair ? 256 : 512) / P.n_mma;
+  if (per_group > 16) per_group = 16;
+  if (per_group > P.n_mtiles) per_group = P.n_mtiles;
+  // as few groups as TMEM allows, then equal shares (14 tiles: 7 + 7, not 8 + 6)
+  const int n_groups = (P.n_mtiles + per_group - 1) / per_group;
+  per_group = (P.n_mtiles + n_groups - 1) / n_groups;
+  P.tiles_per_group = per_group;
+  P.n_groups = (P.n_mtiles + per_group - 1) / per_group;
+  // row splits: the caller's split_k_slices, else about one CTA per SM (two
+  // per SM in the pair layout)
+  const int ctas = (pair ? 2 : 1) * num_sms;
+  int splits = a.split_k > 0 ? a.split_k : (ctas + P.n_groups - 1) / P.n_groups;
+  if (splits > P.n_chunks) splits = P.n_chunks;
+  P.chunks_per_cta = (P.n_chunks + splits - 1) / splits;
+  splits = (P.n_chunks + P.chunks_per_cta - 1) / P.chunks_per_cta;
   P.stages = stages;
   P.bbuf_off = P.stage_bytes * stages;
   P.idx_off = P.bbuf_off + bbuf_bytes;
-  P.bar_off = P.idx_off + idx_total;
+  P.bar_off = P.idx_off + P.idx_buf_bytes * kIdxStages;
   const size_t smem = 1024 + P.bar_off + bar_bytes;
   uint32_t cols = 32;
   while (cols < static_cast<uint32_t>(per_group * P.n_mma)) cols <<= 1;
   P.tmem_cols = cols;
   P.idesc = make_idesc(128, P.n_mma, a.in_dtype == 12 ? 1u : 0u, true, true);
-  void (*kern)(WParams) = gather ? conv_wgrad_kernel<true> : conv_wgrad_kernel<false>;
+  void (*kern)(WParams) = pair     ? conv_wgrad_kernel<true, true>
+                          : gather ? conv_wgrad_kernel<true, false>
+                                   : conv_wgrad_kernel<false, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   dim3 grid(splits, P.n_groups);
-  kern<<<grid, kThreads, smem, stream>>>(P);
+  kern<<<grid, pair ? Layout<true>::kThreads : Layout<false>::kThreads, smem, stream>>>(P);
   return cudaGetLastError();
 }
 
