@@ -52,7 +52,7 @@ struct Meta {
   int n_active;
   uint32_t tilemask;
   int tile;  // tile index of this ring slot, -1 = no more tiles
-  uint32_t grp[4];
+  uint32_t sub[4];  // offsets active in each 32-row group (sub-tile mask, filtered)
   int k_list[32];
 };
 
@@ -73,6 +73,7 @@ struct KParams {
   uint32_t tmem_cols;
   uint32_t idesc;
   int row_bytes;  // bytes of one operand row in a stage: 128 (SWIZZLE_128B) or 64 (SWIZZLE_64B)
+  int bulk_idx;   // sorted index table copied by 512-byte bulk copies (16-byte aligned rows)
 };
 
 __device__ __forceinline__ void flag_error(int *err, int bits) { atomicOr(err, bits); }
@@ -256,6 +257,7 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
     // kLoadWarps warps, kRowsPer rows of the tile per thread (row t + i * 32 kLoadWarps)
     const int t = threadIdx.x - kLoadWarp0 * 32;
     const int lw = t >> 5;
+    int next_draw = 0;  // lane 0 of loader warp 0: the counter value drawn one tile ahead
     for (int it = 0;; ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
@@ -279,9 +281,12 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
         int t = -1;
         if (lane == 0) {
           const int64_t d = A.tile_counter
-                                ? static_cast<int64_t>(atomicAdd(A.tile_counter, 1))
+                                ? static_cast<int64_t>(it == 0 ? atomicAdd(A.tile_counter, 1) : next_draw)
                                 : static_cast<int64_t>(blockIdx.x) + static_cast<int64_t>(it) * gridDim.x;
           t = d < P.num_tiles ? static_cast<int>(d) : -1;
+          // the following tile is drawn now, so the atomic's round trip
+          // overlaps this tile's loads
+          if (A.tile_counter && t >= 0) next_draw = atomicAdd(A.tile_counter, 1);
           sched_tile[it & 3] = t;
           mbar_arrive(&sched_bar[it & 3]);
         }
@@ -301,8 +306,22 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
       const int64_t tile_m = tile / A.n_tiles;
       const int n_tile = static_cast<int>(tile % A.n_tiles);
       uint32_t g0 = 0, g1 = 0, g2 = 0, g3 = 0, tm = 0;
+      // Sorted table and whole 128-row tile with 16-byte aligned slices:
+      // each offset's 128 indices are one 512-byte bulk copy that completes
+      // on idx_full, and the producers apply the sub-tile masks; otherwise
+      // every thread loads, gates and stores its rows' indices.
+      const bool bulk = kGather && P.bulk_idx && (tile_m + 1) * kTileM <= A.M;
+      if (bulk && lw == 0) {
+        if (lane == 0) mbar_expect_tx(&idx_full[b], static_cast<uint32_t>(A.kv) * kTileM * 4);
+        __syncwarp();
+        if (lane < A.kv)
+          bulk_copy_g2s(smem_u32(tab + lane * kTileM),
+                        A.idx_sorted + static_cast<int64_t>(lane) * A.M + tile_m * kTileM, kTileM * 4,
+                        &idx_full[b]);
+      }
 #pragma unroll 1
       for (int rr = 0; rr < kRowsPer; ++rr) {
+        if (bulk && rr > 0) break;
         const int r = t + rr * (kLoadWarps * 32);  // row inside the tile
         const int64_t row_g = tile_m * kTileM + r;
         const bool valid = row_g < A.M;
@@ -311,7 +330,8 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
         // trip per row.  With the sorted table row_g is already the sorted row;
         // otherwise sigma(row) comes first (argsort), then the kv loads.
         int pre[32];
-        if (A.idx_sorted) {
+        if (bulk) {
+        } else if (A.idx_sorted) {
 #pragma unroll
           for (int k = 0; k < 32; ++k)
             pre[k] = (valid && k < A.kv) ? __ldg(A.idx_sorted + static_cast<int64_t>(k) * A.M + row_g)
@@ -375,16 +395,20 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
         // tab[k][r]: index of row r for offset k (-1 where the row's sub-tile
         // mask lacks k).  Written for every offset, whatever the tile mask: a
         // select, not a branch, so no load is deferred to its use.
+        if (!bulk) {
 #pragma unroll
-        for (int k = 0; k < 32; ++k) {
-          if (k < A.kv) {
-            int v = ((sub >> k) & 1u) ? pre[k] : -1;
-            if (v < -1 || v >= A.a_rows) {
-              flag_error(A.err, kErrBadIndex);
-              v = -1;
+          for (int k = 0; k < 32; ++k) {
+            if (k < A.kv) {
+              int v = ((sub >> k) & 1u) ? pre[k] : -1;
+              if (v < -1 || v >= A.a_rows) {
+                flag_error(A.err, kErrBadIndex);
+                v = -1;
+              }
+              tab[k * kTileM + r] = v;
             }
-            tab[k * kTileM + r] = v;
           }
+          // a later bulk copy (async proxy) may overwrite these stores
+          fence_proxy_async_smem();
         }
       }
       if (t == 0) {
@@ -399,6 +423,16 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
         meta->n_active = na;
         meta->tilemask = tm;
         meta->tile = tile;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          uint32_t sq;
+          if (A.tile_m_desp == 32) sq = q == 0 ? g0 : q == 1 ? g1 : q == 2 ? g2 : g3;
+          else if (A.tile_m_desp == 64) sq = q < 2 ? (g0 | g1) : (g2 | g3);
+          else sq = g0 | g1 | g2 | g3;
+          sq &= A.mask_filter;
+          if (A.reverse) sq = __brev(sq) >> (32 - A.kv);
+          meta->sub[q] = sq;
+        }
         meta->nchunks = P.cpo > 0 ? na * P.cpo : (na + P.opc - 1) / P.opc;
       }
       mbar_arrive(&idx_full[b]);
@@ -462,7 +496,16 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
         }
         __syncwarp();
         if (lane < (kTileM / kProdWarps) / 4) {
-          const int4 q = *reinterpret_cast<const int4 *>(tab + k * kTileM + r0);
+          int4 q = *reinterpret_cast<const int4 *>(tab + k * kTileM + r0);
+          // rows r0..r0+3 share a 32-row group: gate by its sub-tile mask
+          // (bulk-copied tables are ungated) and check the indices
+          if (!((meta->sub[r0 >> 5] >> k) & 1u)) q = make_int4(-1, -1, -1, -1);
+          const bool bad = q.x < -1 || q.x >= A.a_rows || q.y < -1 || q.y >= A.a_rows ||
+                           q.z < -1 || q.z >= A.a_rows || q.w < -1 || q.w >= A.a_rows;
+          if (bad) {
+            flag_error(A.err, kErrBadIndex);
+            q = make_int4(-1, -1, -1, -1);
+          }
           tma_gather4(sA + r0 * rb, &P.tmap_a, cb * box, q.x, q.y, q.z, q.w, &full_bar[s]);
         }
         ++gchunk;
@@ -771,6 +814,8 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
   // and filled with cp.async
   bool tma = false, gather = false;
   P.row_bytes = 128;
+  P.bulk_idx = a.idx_sorted != nullptr && reinterpret_cast<uintptr_t>(a.idx_sorted) % 16 == 0 &&
+               a.M % 4 == 0;
   if (a.a_row_bytes == 64 && a.kv > 1 && a.a_rows > 0 &&
       encode_tmap_2d(&P.tmap_b, a.in_dtype, a.b_base, red * a.kv, a.n_total,
                      static_cast<uint64_t>(a.b_row_stride), 64u / esz, a.BN, 64) &&

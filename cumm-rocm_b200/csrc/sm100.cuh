@@ -115,6 +115,23 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
       "r"(bytes)
       : "memory");
 }
+// Add `bytes` to the transaction count of `bar`'s current phase without
+// arriving (the thread arrives later, after its own shared-memory writes).
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Untiled bulk copy global -> shared of `bytes` (both addresses 16-byte
+// aligned, bytes a multiple of 16), completing on `bar`'s transaction count.
+__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void *src, uint32_t bytes,
+                                              uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          dst),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
 // 2-D tiled tensor load of one box at (x, y); x * element size must be a
 // multiple of 16 bytes.
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const void *tmap, int x, int y,
