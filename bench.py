@@ -310,12 +310,15 @@ def run_b200(args, rank, world, dist):
     cmt = ConvMainUnitTest()
     # Steps are pipelined over three streams (uploads, compute, downloads):
     # step s+1's inputs go up while step s computes and step s-1's results
-    # come down; two device and two pinned host buffer sets alternate.
-    # Every step still copies its inputs in and its results out inside the
-    # timed region.
+    # come down.  Step s reuses the device and pinned host buffers of step
+    # s - NBUF once that step's results are down; with two sets the upload ->
+    # compute -> download chain of one step would pace every second step, with
+    # three the host link is the limit.  Every step still copies its inputs in
+    # and its results out inside the timed region.
+    NBUF = 3
     s_in, s_comp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
     bufs = []
-    for _ in range(2):
+    for _ in range(NBUF):
         bufs.append({
             "cd": torch.empty_like(coords_h, device=dev), "xd": torch.empty_like(x_h, device=dev),
             "dyd": torch.empty_like(dy_h, device=dev),
@@ -331,9 +334,9 @@ def run_b200(args, rank, world, dist):
         })
 
     def e2e_step(step: int):
-        b = bufs[step % 2]
+        b = bufs[step % NBUF]
         with torch.cuda.stream(s_in):
-            if step >= 2:
+            if step >= NBUF:
                 s_in.wait_event(b["ev_free"])
             b["cd"].copy_(coords_h, non_blocking=True)
             b["xd"].copy_(x_h, non_blocking=True)
@@ -341,7 +344,7 @@ def run_b200(args, rank, world, dist):
             b["ev_in"].record(s_in)
         with torch.cuda.stream(s_comp):
             s_comp.wait_event(b["ev_in"])
-            if step >= 2:
+            if step >= NBUF:
                 s_comp.wait_event(b["ev_free"])
             cptr = s_comp.cuda_stream
             ptd = build_pair_table(b["cd"], vg.KITTI_SHAPE)
@@ -381,7 +384,7 @@ def run_b200(args, rank, world, dist):
             b["ev_free"].record(s_out)
 
     n_e2e = 0 if args.no_e2e else max(3, min(args.steps, 20))
-    for st in range(2 if n_e2e else 0):
+    for st in range(NBUF if n_e2e else 0):
         e2e_step(st)
     torch.cuda.synchronize()
     if dist is not None:
@@ -448,7 +451,7 @@ def run_b200(args, rank, world, dist):
             "e2e": None if n_e2e == 0 else {
                 "value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                "steps": n_e2e, "pipelined_streams": 3},
+                "steps": n_e2e, "pipelined_streams": 3, "buffer_sets": NBUF},
             "cpu_baseline": cpu,
             "gpu_launches": 5 * args.steps,
             "clocks": clocks,
