@@ -411,7 +411,14 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     e = scb::launch_conv_rowgather(a, sms, s);
     if (e != cudaSuccess) return cuda_fail(e, "conv row-gather launch");
   } else {
-    e = cudaMemsetAsync(p->workspace, 0, p->K * p->kv * p->C * 4, s);
+    // dW = 1 * sum with beta = 0 into an fp32 [K, kv, C] weight covering every
+    // offset: the kernel accumulates straight into dW (bit-identical to the
+    // workspace + finalize route, which computes alpha * ws with alpha = 1)
+    const uint32_t all_offsets = p->kv >= 32 ? 0xffffffffu : ((1u << p->kv) - 1u);
+    const bool direct = p->dtype_weight == SC_FLOAT32 && p->alpha == 1.f && p->beta == 0.f &&
+                        (p->mask_filter & all_offsets) == all_offsets;
+    float *acc = static_cast<float *>(direct ? p->weight : p->workspace);
+    e = cudaMemsetAsync(acc, 0, p->K * p->kv * p->C * 4, s);
     if (e != cudaSuccess) return cuda_fail(e, "zero workspace");
     scb::ConvWgradArgs a{};
     a.dout = static_cast<const uint8_t *>(p->output);
@@ -430,7 +437,7 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     a.mask_filter = p->mask_filter;
     a.argsort = p->mask_argsort;
     a.indices = p->indices;
-    a.ws = static_cast<float *>(p->workspace);
+    a.ws = acc;
     a.err = err;
     a.b_inds = nullptr;
     a.idx_sorted = p->indices_sorted;
@@ -438,6 +445,10 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     a.split_k = p->split_k_slices > 1 ? p->split_k_slices : 0;
     e = scb::launch_conv_wgrad(a, sms, s);
     if (e != cudaSuccess) return cuda_fail(e, "conv wgrad launch");
+    if (direct) {
+      if (p->flags & SC_FLAG_SYNC_CHECK) return sync_check(s);
+      return SC_OK;
+    }
     scb::EpiParams ep{};
     ep.alpha = p->alpha;
     ep.beta = p->beta;
