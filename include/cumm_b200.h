@@ -191,7 +191,9 @@ int sc_conv_workspace_size(const sc_conv_params *p, int64_t *bytes);
  * Same params and results as sc_conv_implicit_gemm with op_type
  * SC_CONV_BACKWARD_WEIGHT; workspace must be NULL / 0.  The fp32 [K, kv, C]
  * accumulator lives in a static 8 MiB device array of this library, so
- * K * kv * C must be <= 2097152 (else SC_INVALID_ARG).  Nothing has to start
+ * K * kv * C must be <= 2097152 (else SC_INVALID_ARG); an fp32 dW with
+ * alpha 1, beta 0 and every offset in mask_filter is accumulated in dW itself
+ * and leaves the array untouched.  Nothing has to start
  * at zero: each call clears the part it uses on p->stream before the kernel.
  * The first call on a device (with that device current) looks up the array's
  * address; make that first call before any stream capture starts.  There is
