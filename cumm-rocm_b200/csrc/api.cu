@@ -363,17 +363,6 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     a.a_rows = fwd ? p->n_in : p->n_out;
     a.a_row_bytes = static_cast<int>(red * es);
     a.a_row_stride = red * es;
-    if (fwd) {
-      a.b_base = static_cast<const uint8_t *>(p->weight);
-    } else {
-      e = scb::launch_transpose_weight(p->weight, ws + kSchedBytes, static_cast<int>(p->K), p->kv,
-                                       static_cast<int>(p->C), es, s);
-      if (e != cudaSuccess) return cuda_fail(e, "weight transpose launch");
-      a.b_base = ws + kSchedBytes;
-    }
-    a.b_row_stride = static_cast<int64_t>(p->kv) * red * es;
-    a.b_off_stride = static_cast<int>(red * es);
-    a.n_total = static_cast<int>(ncols);
     int tiles = 1;
     int64_t bn = ncols;
     if (p->tile_n > 0) {
@@ -386,6 +375,23 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
         bn = ncols / tiles;
       }
     }
+    // backward-input reads the weight MN-major when the slabs are whole
+    // 64 x 64 boxes of 16-bit data, else from a transposed [C, kv, K] copy
+    const bool b_mn = !fwd && es == 2 && red % 64 == 0 && bn % 64 == 0 && p->n_out > 0 &&
+                      reinterpret_cast<uintptr_t>(p->weight) % 16 == 0;
+    if (fwd || b_mn) {
+      a.b_base = static_cast<const uint8_t *>(p->weight);
+    } else {
+      e = scb::launch_transpose_weight(p->weight, ws + kSchedBytes, static_cast<int>(p->K), p->kv,
+                                       static_cast<int>(p->C), es, s);
+      if (e != cudaSuccess) return cuda_fail(e, "weight transpose launch");
+      a.b_base = ws + kSchedBytes;
+    }
+    a.b_mn = b_mn ? 1 : 0;
+    // B rows: [n, kv, red] (K-major), or for b_mn the weight's [red, kv, n]
+    a.b_row_stride = static_cast<int64_t>(p->kv) * (b_mn ? ncols : red) * es;
+    a.b_off_stride = static_cast<int>((b_mn ? ncols : red) * es);
+    a.n_total = static_cast<int>(ncols);
     a.BN = static_cast<int>(bn);
     a.n_tiles = tiles;
     a.M = p->N;

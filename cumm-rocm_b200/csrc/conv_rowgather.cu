@@ -74,6 +74,7 @@ struct KParams {
   uint32_t idesc;
   int row_bytes;  // bytes of one operand row in a stage: 128 (SWIZZLE_128B) or 64 (SWIZZLE_64B)
   int bulk_idx;   // sorted index table copied by 512-byte bulk copies (16-byte aligned rows)
+  int b_mn;       // weight slab is MN-major: BN / 64 boxes of 64 reduction rows x 64 columns
 };
 
 __device__ __forceinline__ void flag_error(int *err, int bits) { atomicOr(err, bits); }
@@ -488,8 +489,15 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
         if (lane == 0) {
           if (static_cast<int>(gchunk % kProdWarps) == pw) {
             mbar_arrive_expect_tx(&full_bar[s], a_tx + b_tx);
-            tma_load_2d(sA + P.b_off, &P.tmap_b, k * (A.b_off_stride / esz) + cb * box, n0,
-                        &full_bar[s]);
+            if (P.b_mn) {
+              // rows j = cb * 64 .. + 63 of the weight, columns k * C + n0 + 64 q
+              for (int q = 0; q < A.BN / 64; ++q)
+                tma_load_2d(sA + P.b_off + q * 8192, &P.tmap_b, k * (A.b_off_stride / esz) + n0 + 64 * q,
+                            cb * 64, &full_bar[s]);
+            } else {
+              tma_load_2d(sA + P.b_off, &P.tmap_b, k * (A.b_off_stride / esz) + cb * box, n0,
+                          &full_bar[s]);
+            }
           } else {
             mbar_arrive_expect_tx(&full_bar[s], a_tx);
           }
@@ -656,6 +664,12 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
       const uint64_t a_desc0 = P.row_bytes == 64 ? make_sdesc_l(smem_base, 16, 512, 4u)
                                                  : make_sdesc(smem_base, 16, 1024);
       const int mmas = P.row_bytes / 32;
+      // B of stage 0 and its step per MMA (descriptor units of 16 bytes):
+      // K-major B advances 32 bytes inside its rows; MN-major B (64-wide
+      // column atoms 8 KB apart) advances 16 rows = 2 KB
+      const uint64_t b_desc0 = P.b_mn ? make_sdesc(smem_base + P.b_off, 8192, 1024)
+                                      : a_desc0 + static_cast<uint64_t>(P.b_off >> 4);
+      const uint64_t b_kstep = P.b_mn ? 128 : 2;
       for (;; ++it) {
         const int b = it % kIdxStages;
         const uint32_t ph = (it / kIdxStages) & 1;
@@ -695,13 +709,13 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
           }
           tc_fence_after();
           const uint64_t ad0 = a_desc0 + static_cast<uint64_t>((s * P.stage_bytes) >> 4);
-          const uint64_t bd0 = ad0 + static_cast<uint64_t>(P.b_off >> 4);
+          const uint64_t bd0 = b_desc0 + static_cast<uint64_t>((s * P.stage_bytes) >> 4);
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk) {
             if (kk >= mmas) break;
             // K advances 32 bytes inside the swizzle atom (start address >> 4)
             const uint64_t ad = ad0 + static_cast<uint64_t>(kk * 2);
-            const uint64_t bd = bd0 + static_cast<uint64_t>(kk * 2);
+            const uint64_t bd = bd0 + static_cast<uint64_t>(kk) * b_kstep;
             if constexpr (kF8)
               mma_f8(d, ad, bd, P.idesc, (j | kk) != 0 ? 1u : 0u);
             else
@@ -836,15 +850,22 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
     P.upo = a.a_row_bytes / 16;
   }
   // TMA weight slabs: whole 128-byte reduction chunks (no packing of small offsets)
+  P.b_mn = a.b_mn;
   if (P.cpo > 0 && P.row_bytes == 128) {
     const uint32_t box = 128u / esz;
-    tma = encode_tmap_2d(&P.tmap_b, a.in_dtype, a.b_base, red * a.kv, a.n_total,
-                         static_cast<uint64_t>(a.b_row_stride), box, a.BN);
+    // MN-major weight: [red rows, kv * n_total columns], 64 x 64 boxes
+    tma = a.b_mn ? encode_tmap_2d(&P.tmap_b, a.in_dtype, a.b_base,
+                                  static_cast<uint64_t>(a.n_total) * a.kv, red,
+                                  static_cast<uint64_t>(a.b_row_stride), 64, 64)
+                 : encode_tmap_2d(&P.tmap_b, a.in_dtype, a.b_base, red * a.kv, a.n_total,
+                                  static_cast<uint64_t>(a.b_row_stride), box, a.BN);
     // gathered A rows: [a_rows, red] with one-row boxes (tile::gather4)
     if (tma && a.a_row_bytes >= 128 && a.a_rows > 0)
       gather = encode_tmap_2d(&P.tmap_a, a.in_dtype, a.a_base, red, static_cast<uint64_t>(a.a_rows),
                               static_cast<uint64_t>(a.a_row_stride), box, 1);
   }
+  // the MN-major weight slab is only read by the TMA gather path
+  if (a.b_mn && (!gather || a.BN % 64 != 0 || esz != 2)) return cudaErrorInvalidConfiguration;
   const uint32_t a_bytes = kTileM * static_cast<uint32_t>(P.row_bytes);
   const uint32_t b_bytes = static_cast<uint32_t>(a.BN) * P.row_bytes;
   P.stage_bytes = a_bytes + b_bytes;
@@ -883,7 +904,7 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
       default: return launch_typed<true, __nv_bfloat16>(P, tma, gather, pair, grid, smem, stream);
     }
   }
-  P.idesc = make_idesc(128, a.BN, a.in_dtype == 12 ? 1u : 0u, false, false);
+  P.idesc = make_idesc(128, a.BN, a.in_dtype == 12 ? 1u : 0u, false, a.b_mn != 0);
   switch (a.out_dtype) {
     case 0: return launch_typed<false, float>(P, tma, gather, pair, grid, smem, stream);
     case 7: return launch_typed<false, __half>(P, tma, gather, pair, grid, smem, stream);

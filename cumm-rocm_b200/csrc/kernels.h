@@ -53,6 +53,11 @@ struct ConvRowGatherArgs {
   int64_t out_rows;          // bound for output rows
   const int32_t *idx_sorted; // optional [kv, M]: indices[k][argsort[r]]
   int *tile_counter;         // optional, zero at launch: tiles handed out dynamically
+  // backward-input with B = the [K, kv, C] weight itself: the slab of offset
+  // k is rows j (reduction) x columns k * C + c (n), read MN-major by the
+  // tensor core (no transposed copy); needs 16-bit data, red % 64 == 0 and
+  // BN % 64 == 0 on the TMA gather path
+  int b_mn;
 };
 cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaStream_t stream);
 
