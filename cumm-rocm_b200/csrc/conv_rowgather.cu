@@ -23,13 +23,17 @@
 //                    mask_argsort[r] (permuted store)
 //   producer warps   A rows of each (offset, 128-byte column block) chunk by
 //                    TMA tile::gather4 (4 rows per lane, SWIZZLE_128B or
-//                    SWIZZLE_64B by address; index -1 reads as zero rows) and
-//                    the weight slab by one 2-D TMA box; shorter rows (16 / 32
-//                    bytes, several offsets packed per 128-byte row) by 16-byte
-//                    cp.async instead
+//                    SWIZZLE_64B by address; index -1 reads as zero rows, each
+//                    group of 4 gated by its 32-row sub-tile mask) and the
+//                    weight slab by 2-D TMA boxes (backward-input: the [K, kv,
+//                    C] weight itself, read MN-major); shorter rows (16 / 32
+//                    bytes, several offsets packed per 128-byte row) by
+//                    16-byte cp.async instead
 //   loader warps     tile masks (OR, mask_filter, brev for backward-input),
 //                    mask_output, and the tile's [offset][row] index table into
-//                    a shared-memory ring, all loads of a row issued together
+//                    a shared-memory ring: with the sorted table one 512-byte
+//                    cp.async.bulk per offset, else all loads of a row issued
+//                    together; the next tile is drawn one tile ahead
 //   MMA warp         TMEM allocator + single-thread tcgen05.mma issuer into a
 //                    double-buffered fp32 TMEM accumulator (128 lanes x BN)
 // Layouts (Layout<kPair>): one 17-warp CTA per SM, or on the gather path two
