@@ -262,7 +262,7 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
     // kLoadWarps warps, kRowsPer rows of the tile per thread (row t + i * 32 kLoadWarps)
     const int t = threadIdx.x - kLoadWarp0 * 32;
     const int lw = t >> 5;
-    int next_draw = 0;  // lane 0 of loader warp 0: the counter value drawn one tile ahead
+    int next_draw = -1;  // lane 0 of loader warp 0: counter value drawn one tile ahead, or -1
     for (int it = 0;; ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
@@ -286,12 +286,16 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
         int t = -1;
         if (lane == 0) {
           const int64_t d = A.tile_counter
-                                ? static_cast<int64_t>(it == 0 ? atomicAdd(A.tile_counter, 1) : next_draw)
+                                ? static_cast<int64_t>(next_draw >= 0 ? next_draw : atomicAdd(A.tile_counter, 1))
                                 : static_cast<int64_t>(blockIdx.x) + static_cast<int64_t>(it) * gridDim.x;
           t = d < P.num_tiles ? static_cast<int>(d) : -1;
-          // the following tile is drawn now, so the atomic's round trip
-          // overlaps this tile's loads
-          if (A.tile_counter && t >= 0) next_draw = atomicAdd(A.tile_counter, 1);
+          // While more tiles remain than there are CTAs, the following tile is
+          // drawn now, so the atomic's round trip overlaps this tile's loads;
+          // near the end (or on a grid with few tiles) a CTA holding two
+          // tiles would idle the others, so it draws when it needs one.
+          next_draw = -1;
+          if (A.tile_counter && t >= 0 && d + 2 * static_cast<int64_t>(gridDim.x) < P.num_tiles)
+            next_draw = atomicAdd(A.tile_counter, 1);
           sched_tile[it & 3] = t;
           mbar_arrive(&sched_bar[it & 3]);
         }

@@ -339,5 +339,10 @@ def main(rates=(50, 100, 200, 400, 800), n_req: int = 160, fp8: bool = False, se
 
 
 if __name__ == "__main__":
-    import sys
-    main(fp8="--fp8" in sys.argv)
+    import argparse
+    ap = argparse.ArgumentParser(description="Poisson-arrival serving sweep: plain vs continuous")
+    ap.add_argument("--fp8", action="store_true")
+    ap.add_argument("--rates", default="50,100,200,400,800", help="comma-separated request rates (req/s)")
+    ap.add_argument("--requests", type=int, default=160, help="requests per rate and mode")
+    args = ap.parse_args()
+    main(rates=tuple(int(r) for r in args.rates.split(",")), n_req=args.requests, fp8=args.fp8)
