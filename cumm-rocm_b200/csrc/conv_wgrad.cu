@@ -111,10 +111,25 @@ __device__ __forceinline__ void atom_elem(const WParams &P, int a, int e, int &k
   }
 }
 
+// M-tiles of group g: n_mtiles / n_groups each, and the remainder goes to
+// the outer groups first (0, last, 1, last - 1, ...).  The middle offsets of
+// a kernel carry the most pairs (a submanifold conv's centre and, on surfaces,
+// its in-plane neighbours), so the middle groups get fewer tiles: 14 tiles in
+// 4 groups are 4 + 3 + 3 + 4, not 4 + 4 + 4 + 2.  No group exceeds
+// tiles_per_group (the TMEM columns of a CTA).
 __device__ __forceinline__ void group_filters(const WParams &P, int g, int &k_lo, int &k_hi,
                                               int &t0, int &t1) {
-  t0 = g * P.tiles_per_group;
-  t1 = min(t0 + P.tiles_per_group, P.n_mtiles);
+  const int n = P.n_groups;
+  const int base = P.n_mtiles / n, rem = P.n_mtiles % n;
+  auto size = [&](int q) {
+    const int m = n - 1 - q;
+    const int rank = q < m ? 2 * q : 2 * m + 1;  // order 0, n-1, 1, n-2, ...
+    return base + (rank < rem ? 1 : 0);
+  };
+  int s = 0;
+  for (int q = 0; q < g; ++q) s += size(q);
+  t0 = s;
+  t1 = min(s + size(g), P.n_mtiles);
   const int a0 = 2 * t0;
   const int a1 = min(2 * t1, P.n_atoms);  // exclusive
   if (P.cpa > 0) {
