@@ -95,6 +95,10 @@ int sync_check(cudaStream_t s) {
 
 bool is16(int dt) { return dt == SC_BFLOAT16 || dt == SC_FLOAT16; }
 
+// The tensor-core kernels move whole 16-byte units (TMA boxes and gathers,
+// 16-byte cp.async, uint4 / float4 epilogue loads and stores, v4 reductions).
+bool aligned16(const void *q) { return reinterpret_cast<uintptr_t>(q) % 16 == 0; }
+
 int64_t align256(int64_t x) { return (x + 255) & ~static_cast<int64_t>(255); }
 
 // Reduction row width accepted by the row-gather kernel (bytes per offset).
@@ -169,6 +173,20 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
     return SC_OK;
   }
   if (p->algo != SC_ALGO_TCGEN05) return fail(SC_RUNTIME, "Can't Found Algorithm: unknown algo %d", p->algo);
+  // Every tensor a tcgen05 kernel reads or writes in 16-byte units must start
+  // on a 16-byte boundary; a misaligned view is an argument error here rather
+  // than a misaligned access on the device.  (Backward weight writes dW with
+  // scalar stores unless it can accumulate into it directly, which checks
+  // dW's alignment itself.)
+  {
+    const bool wg = op == SC_CONV_BACKWARD_WEIGHT;
+    const void *need[5] = {p->input, p->output, wg ? nullptr : p->weight, p->bias, p->output_add};
+    const char *names[5] = {"input", "output", "weight", "bias", "output_add"};
+    for (int i = 0; i < 5; ++i)
+      if (!aligned16(need[i]))
+        return fail(SC_INVALID_ARG, "%s must start on a 16-byte boundary for the tcgen05 kernels (address %p)",
+                    names[i], need[i]);
+  }
   if (p->tile_n != 0 && op != SC_CONV_BACKWARD_WEIGHT) {
     const int64_t ncols = op == SC_CONV_FORWARD ? p->K : p->C;
     if (p->tile_n < 16 || p->tile_n > 256 || p->tile_n % 16 || ncols % p->tile_n)
@@ -419,10 +437,12 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
   } else {
     // dW = 1 * sum with beta = 0 into an fp32 [K, kv, C] weight covering every
     // offset: the kernel accumulates straight into dW (bit-identical to the
-    // workspace + finalize route, which computes alpha * ws with alpha = 1)
+    // workspace + finalize route, which computes alpha * ws with alpha = 1).
+    // Its red.global.add.v4.f32 needs a 16-byte aligned dW; any other dW goes
+    // through the workspace and the finalize kernel's scalar stores.
     const uint32_t all_offsets = p->kv >= 32 ? 0xffffffffu : ((1u << p->kv) - 1u);
     const bool direct = p->dtype_weight == SC_FLOAT32 && p->alpha == 1.f && p->beta == 0.f &&
-                        (p->mask_filter & all_offsets) == all_offsets;
+                        (p->mask_filter & all_offsets) == all_offsets && aligned16(p->weight);
     float *acc = static_cast<float *>(direct ? p->weight : p->workspace);
     e = cudaMemsetAsync(acc, 0, p->K * p->kv * p->C * 4, s);
     if (e != cudaSuccess) return cuda_fail(e, "zero workspace");
@@ -482,7 +502,8 @@ static __device__ __align__(256) float g_wgrad_scratch[kStaticScratchFloats];
 float *g_scratch_ptr[kMaxDevices] = {nullptr};
 
 // Address of this device's copy of g_wgrad_scratch, looked up once per device
-// (with that device current) and cached.
+// (with that device current) and cached.  cudaDeviceReset after that first
+// lookup is unsupported: the module would reload at another address.
 int scratch_address(float **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

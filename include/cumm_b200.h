@@ -77,6 +77,9 @@ extern "C" {
  *   mask_argsort [N] int32
  *   mask_output [ceil(N / tile_m)] uint32 (FORWARD writes, BACKWARD_WEIGHT reads
  *   through `mask` with mask_width rows per word)
+ * With SC_ALGO_TCGEN05, input, output, bias, output_add and (forward,
+ * backward-input) weight must start on a 16-byte boundary, else
+ * SC_INVALID_ARG; a backward-weight dW may start at any element.
  */
 typedef struct sc_conv_params {
   int32_t op_type;
@@ -196,7 +199,9 @@ int sc_conv_workspace_size(const sc_conv_params *p, int64_t *bytes);
  * and leaves the array untouched.  Nothing has to start
  * at zero: each call clears the part it uses on p->stream before the kernel.
  * The first call on a device (with that device current) looks up the array's
- * address; make that first call before any stream capture starts.  There is
+ * address and caches it; make that first call before any stream capture
+ * starts, and do not call cudaDeviceReset on that device afterwards (the
+ * module reloads at a new address and the cached one is stale).  There is
  * one array per device: calls that may run at the same time on one device
  * (different streams or host threads) race on it and give wrong gradients;
  * calls queued on one stream are safe.

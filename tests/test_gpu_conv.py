@@ -87,6 +87,62 @@ def test_wgrad_tcgen05(dw_dt, n, grid, C, K):
     _assert_close(to64(dw), ref, TOL_16 if dw_dt == tv.bfloat16 else 2e-5)
 
 
+def test_wgrad_fp32_dw_at_element_offset():
+    """An fp32 dW view that starts 4 bytes past a 16-byte boundary cannot take
+    the in-place accumulation (its v4 reductions need 16-byte alignment); it
+    goes through the workspace and the finalize kernel and gives the aligned
+    result."""
+    n, grid, C, K = 3000, 24, 64, 64
+    coords, pf, pb, m = _subm(n, grid, 21)
+    rng = np.random.default_rng(21)
+    xt = dev(rng.standard_normal((n, C)).astype(np.float32), torch.bfloat16)
+    dyt = dev(rng.standard_normal((n, K)).astype(np.float32), torch.bfloat16)
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    mo = co.tile_masks(ms, 128).astype(np.uint32)
+    desp = find_desp(ConvOpType.kBackwardWeight, "Tcgen05", tv.bfloat16, tv.float32, tv.bfloat16, 128)
+    dw = torch.zeros((K, 27, C), dtype=torch.float32, device="cuda")
+    conv(ConvOpType.kBackwardWeight, desp, xt, dw, dyt, pf, mo, order, mask_width=128)
+    buf = torch.full((K * 27 * C + 1,), 5.0, dtype=torch.float32, device="cuda")
+    dw_off = buf[1:].view(K, 27, C)
+    assert dw_off.data_ptr() % 16 == 4
+    conv(ConvOpType.kBackwardWeight, desp, xt, dw_off, dyt, pf, mo, order, mask_width=128)
+    nr, _, _ = co.rel_err(to64(dw_off), to64(dw))
+    assert nr < 1e-6, nr
+    assert buf[0].item() == 5.0
+    ref = co.conv_wgrad_masked(to64(dyt), to64(xt), pf, mo, 128, order, 27)
+    _assert_close(to64(dw_off), ref, 2e-5)
+
+
+def test_fwd_output_add_scale_bias_epilogue():
+    """The reference's int8-inference epilogue form with a residual operand:
+    out = act(scale * acc + alpha * bias + beta * output_add)
+    (cumm/conv/nvrtc_code.py:78-99, cumm/gemm/output_op/linear.py:300-392;
+    the int8 clamp does not apply to a floating-point output)."""
+    n, grid, C, K = 2500, 20, 64, 64
+    coords, pf, pb, m = _subm(n, grid, 22)
+    rng = np.random.default_rng(22)
+    x = rng.standard_normal((n, C)).astype(np.float32)
+    w = vg.kaiming_uniform(K, 27, C, 22)
+    xt, wt = dev(x, torch.bfloat16), dev(w, torch.bfloat16)
+    scale = dev((0.5 + rng.random(K)).astype(np.float32))
+    bias = dev(rng.standard_normal(K).astype(np.float32), torch.bfloat16)
+    res = dev(rng.standard_normal((n, K)).astype(np.float32), torch.bfloat16)
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 128)
+    for act_type, act_alpha in ((0, 0.0), (1, 0.0), (3, 0.2)):
+        out = torch.full((n, K), 9.0, dtype=torch.bfloat16, device="cuda")
+        conv(ConvOpType.kForward, desp, xt, wt, out, pf, ms, order, alpha=0.75, beta=0.5, bias=bias,
+             scale=scale, output_add=res, act_type=act_type, act_alpha=act_alpha)
+        ref, _ = co.conv_fwd_masked(to64(xt), to64(wt), pf, ms, order, 128, alpha=0.75, beta=0.5,
+                                    bias=to64(bias), scale=to64(scale), output_add=to64(res),
+                                    act_type=act_type, act_alpha=act_alpha)
+        _assert_close(to64(out), ref, TOL_16)
+    # output_add without scale is the reference's "only int8 inference" error
+    out = torch.zeros((n, K), dtype=torch.bfloat16, device="cuda")
+    with pytest.raises(ValueError, match="output_add"):
+        conv(ConvOpType.kForward, desp, xt, wt, out, pf, ms, order, output_add=res)
+
+
 def test_split_two_launches_equals_single():
     """MaskSplitImplicitGemm: split filters with beta=1 on the second launch
     (main_real_spconv.py:273-294) equals one launch with all offsets."""
@@ -258,6 +314,64 @@ def test_lidar_200k_fwd_dgrad_wgrad(seed):
          find_desp(ConvOpType.kBackwardWeight, "Tcgen05", tv.bfloat16, tv.float32, tv.bfloat16, 128),
          xt, dw, dyt, pf, mo.numpy(), order, mask_width=128)
     _assert_close(to64(dw), co.wgrad_gather_gemm_scatter(dy64, x64, pf), TOL_16)
+
+
+def test_lidar_200k_bench_path():
+    """The exact call sequence bench.py times, at its full size, against the
+    FP64 oracle: the GPU pair build, indices_sorted (the forward and
+    backward-input kernels then copy whole tiles' index slices with
+    cp.async.bulk), the forward's mask_output feeding backward-weight, and an
+    fp32 dW accumulated in place (alpha 1, beta 0, every offset)."""
+    from cumm.conv.main import ConvMainUnitTest
+    from cumm.spconv_ops import build_pair_table
+    from cumm.tensorview.gemm import ConvParams
+    n, C, K = 200000, 64, 64
+    coords = vg.lidar_voxels(n, seed=0)
+    pt = build_pair_table(torch.from_numpy(coords).cuda(), vg.KITTI_SHAPE)
+    pf, pb, m = po.subm_pairs(coords, vg.KITTI_SHAPE)
+    assert np.array_equal(pt.pairs_fwd.cpu().numpy(), pf)
+    assert np.array_equal(pt.pairs_bwd.cpu().numpy(), pb)
+    rng = np.random.default_rng(0)
+    xt = dev(rng.standard_normal((n, C)).astype(np.float32), torch.bfloat16)
+    dyt = dev(rng.standard_normal((n, K)).astype(np.float32), torch.bfloat16)
+    wt = dev(vg.kaiming_uniform(K, 27, C, 0), torch.bfloat16)
+    out = torch.empty((n, K), dtype=torch.bfloat16, device="cuda")
+    din = torch.empty((n, C), dtype=torch.bfloat16, device="cuda")
+    dw = torch.full((K, 27, C), 3.0, dtype=torch.float32, device="cuda")
+    mo = torch.empty(((n + 127) // 128,), dtype=torch.int32, device="cuda")
+    for op in (ConvOpType.kForward, ConvOpType.kBackwardInput, ConvOpType.kBackwardWeight):
+        p = ConvParams(3, op)
+        p.conv_algo_desp = find_desp(op, "Tcgen05", tv.bfloat16,
+                                     tv.float32 if op == ConvOpType.kBackwardWeight else tv.bfloat16,
+                                     tv.bfloat16, 128)
+        if op == ConvOpType.kForward:
+            p.input, p.weight, p.output = tv.Tensor(xt), tv.Tensor(wt), tv.Tensor(out)
+            p.indices = tv.Tensor(pt.pairs_fwd)
+            p.mask = tv.Tensor(pt.masks_fwd[0], tv.uint32)
+            p.mask_output = tv.Tensor(mo, tv.uint32)
+        elif op == ConvOpType.kBackwardInput:
+            p.input, p.weight, p.output = tv.Tensor(din), tv.Tensor(wt), tv.Tensor(dyt)
+            p.indices = tv.Tensor(pt.pairs_bwd)
+            p.mask = tv.Tensor(pt.masks_fwd[0], tv.uint32)
+            p.reverse_mask = True
+        else:
+            p.input, p.weight, p.output = tv.Tensor(xt), tv.Tensor(dw), tv.Tensor(dyt)
+            p.indices = tv.Tensor(pt.pairs_fwd)
+            p.mask = tv.Tensor(mo, tv.uint32)
+            p.mask_width = 128
+        p.mask_argsort = tv.Tensor(pt.argsorts_fwd[0])
+        p.indices_sorted = tv.Tensor(pt.sorted_indices("bwd" if op == ConvOpType.kBackwardInput else "fwd"))
+        ConvMainUnitTest(sync_check=True).implicit_gemm2(p)
+    torch.cuda.synchronize()
+    ms = pt.masks_fwd[0].cpu().numpy().view(np.uint32)
+    order = pt.argsorts_fwd[0].cpu().numpy()
+    x64, w64, dy64 = to64(xt), to64(wt), to64(dyt)
+    ref, mo_ref = co.conv_fwd_masked(x64, w64, pf, ms, order, 128)
+    _assert_close(to64(out), ref, TOL_16)
+    assert np.array_equal(mo.cpu().numpy().view(np.uint32), mo_ref)
+    _assert_close(to64(din), co.dgrad_gather_gemm_scatter(dy64, w64, pb), TOL_16)
+    _assert_close(to64(dw), co.wgrad_gather_gemm_scatter(dy64, x64, pf), TOL_16)
+    _assert_close(to64(dw), co.conv_wgrad_masked(dy64, x64, pf, mo_ref, 128, order, 27), TOL_16)
 
 
 @pytest.mark.parametrize("n", [30000, 30001])

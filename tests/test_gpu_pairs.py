@@ -5,6 +5,7 @@ import torch
 
 from cumm import voxelgen as vg
 from cumm.spconv_ops import SpconvOps, build_pair_table
+from oracle import conv_oracle as co
 from oracle import pairs_oracle as po
 
 pytestmark = pytest.mark.gpu
@@ -70,3 +71,35 @@ def test_sort_large_keys_stable():
         s, o = po.sort_by_key_split(data, sm)
         assert np.array_equal(order.cpu().numpy(), o)
         assert np.array_equal(tt.cpu().numpy().view(np.uint32), s)
+
+
+@pytest.mark.parametrize("n,seed,dil", [(20000, 6, 1), (5000, 7, 2)])
+def test_subm_invariants_the_reference_caller_relies_on(n, seed, dil):
+    """Properties of a submanifold pair table that the reference's driver
+    depends on (cumm/conv/main_real_spconv.py:79-105): every voxel is its own
+    centre neighbour, so the centre bit 1 << (kv // 2) is set in every mask
+    (the driver seeds the split masks with it, :83-84) and the centre column
+    is the identity; the table is symmetric, pairs_bwd[k] == pairs_fwd[kv-1-k]
+    (offset k from an output is offset kv-1-k from its input, which is what
+    lets backward-input reuse the forward's masks with reverse_mask); and the
+    mask bit k is set exactly where pairs_fwd[k] != -1."""
+    coords = vg.lidar_voxels(n, seed=seed)
+    pt = build_pair_table(torch.from_numpy(coords).cuda(), vg.KITTI_SHAPE,
+                          dilation=(dil, dil, dil))
+    pf = pt.pairs_fwd.cpu().numpy()
+    pb = pt.pairs_bwd.cpu().numpy()
+    kv = pf.shape[0]
+    assert kv == 27
+    assert np.array_equal(pb, pf[::-1])
+    assert np.array_equal(pf[kv // 2], np.arange(n, dtype=np.int32))
+    order = pt.argsorts_fwd[0].cpu().numpy()
+    ms = _u(pt.masks_fwd[0])
+    assert np.all(ms & np.uint32(1 << (kv // 2)))
+    m = np.zeros(n, np.uint32)
+    m[order] = ms
+    bits = ((m[None, :] >> np.arange(kv, dtype=np.uint32)[:, None]) & 1).astype(bool)
+    assert np.array_equal(bits, pf >= 0)
+    # the reverse-mask relation: brev(mask) >> (32 - kv) is the mask of pairs_bwd
+    rev = co.brev_shift(m, kv)
+    bits_b = ((rev[None, :] >> np.arange(kv, dtype=np.int64)[:, None]) & 1).astype(bool)
+    assert np.array_equal(bits_b, pb >= 0)

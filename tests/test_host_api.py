@@ -81,6 +81,33 @@ def test_conv_validation_codes():
         _lib.check(_lib.SC_RUNTIME)
 
 
+def test_misaligned_tensors_rejected_before_launch():
+    """A tensor view that does not start on a 16-byte boundary is an argument
+    error of the tcgen05 path (its kernels move 16-byte units), reported by the
+    host checks before any device access: these dummy pointers are never
+    dereferenced."""
+    lib = _lib.load()
+    for op, field in ((0, "input"), (0, "weight"), (0, "output"), (1, "input"), (1, "weight"),
+                      (1, "output"), (2, "input"), (2, "output")):
+        cp = _fake_conv(op, **{field: 0x1000 + 4})
+        rc, _, msg = _ws(cp)
+        assert rc == _lib.SC_INVALID_ARG and "16-byte boundary" in msg and field in msg, (op, field, msg)
+        cp.workspace, cp.workspace_bytes = 0x100000, 1 << 24
+        assert lib.sc_conv_implicit_gemm(ctypes.byref(cp)) == _lib.SC_INVALID_ARG, (op, field)
+    rc, _, msg = _ws(_fake_conv(0, bias=0x2000 + 8))
+    assert rc == _lib.SC_INVALID_ARG and "bias" in msg
+    # backward weight may write a dW view at any 4-byte offset (scalar stores
+    # through the workspace and the finalize kernel)
+    cp = _fake_conv(2, weight=0x1000 + 4)
+    cp.dtype_weight = tv.float32
+    assert _ws(cp)[0] == 0
+    # the fp32 SIMT path reads scalars only
+    cp = _fake_conv(0, input=0x1000 + 4)
+    cp.algo = _lib.SC_ALGO_SIMT
+    cp.dtype_input = cp.dtype_weight = cp.dtype_output = tv.float32
+    assert _ws(cp)[0] == 0
+
+
 def test_null_params():
     lib = _lib.load()
     assert lib.sc_conv_implicit_gemm(None) == _lib.SC_INVALID_ARG

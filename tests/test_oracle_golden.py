@@ -138,3 +138,23 @@ def test_epilogue_ops():
     bias = rng.standard_normal(4)
     v = co.epilogue(acc, rows, prev, 2.0, 0.5, co.ACT_RELU, scale=scale, bias=bias)
     np.testing.assert_allclose(v, np.maximum(scale * acc + 2.0 * bias + 0.5 * prev[rows], 0))
+
+
+def test_subm_invariants_oracle_builder():
+    """The oracle pair builder keeps the submanifold invariants the reference
+    driver relies on (cumm/conv/main_real_spconv.py:79-105): centre bit set in
+    every mask, identity centre column, pairs_bwd[k] == pairs_fwd[kv-1-k], and
+    brev(mask) >> (32 - kv) marking exactly the pairs of pairs_bwd."""
+    from cumm import voxelgen as vg
+    coords = vg.lidar_voxels(6000, seed=3)
+    for dil in (1, 2):
+        pf, pb, m = po.subm_pairs(coords, vg.KITTI_SHAPE, dilation=(dil, dil, dil))
+        kv = pf.shape[0]
+        assert np.array_equal(pb, pf[::-1])
+        assert np.array_equal(pf[kv // 2], np.arange(coords.shape[0], dtype=np.int32))
+        assert np.all(m.astype(np.int64) & (1 << (kv // 2)))
+        bits = ((m.astype(np.int64)[None, :] >> np.arange(kv)[:, None]) & 1).astype(bool)
+        assert np.array_equal(bits, pf >= 0)
+        rev = co.brev_shift(m, kv)
+        bits_b = ((rev[None, :] >> np.arange(kv)[:, None]) & 1).astype(bool)
+        assert np.array_equal(bits_b, pb >= 0)
