@@ -630,6 +630,56 @@ int sc_gemm_matmul(const sc_gemm_params *p) {
   return SC_OK;
 }
 
+// ------------------------------------------------------------------ gather / scatter
+static int check_rows_args(const void *out, const void *in, const int32_t *indices, int64_t m,
+                           int64_t row_bytes, int32_t bpa, int32_t threads) {
+  if (m < 0 || row_bytes < 0) return fail(SC_INVALID_ARG, "bad m / row size");
+  if (bpa != 4 && bpa != 8 && bpa != 16)
+    return fail(SC_INVALID_ARG, "bytes_per_access %d must be 4, 8 or 16", bpa);
+  if (threads != 64 && threads != 128 && threads != 256)
+    return fail(SC_INVALID_ARG, "num_threads %d must be 64, 128 or 256", threads);
+  if (row_bytes % bpa) return fail(SC_RUNTIME, "not supported. use supported() to check first");
+  if (m > 0 && row_bytes > 0 && (out == nullptr || in == nullptr || indices == nullptr))
+    return fail(SC_INVALID_ARG, "output, input and indices must not be empty");
+  if (reinterpret_cast<uintptr_t>(out) % bpa || reinterpret_cast<uintptr_t>(in) % bpa)
+    return fail(SC_INVALID_ARG, "output and input must be aligned to bytes_per_access (%d)", bpa);
+  return SC_OK;
+}
+
+int sc_gather_rows(void *out, const void *in, int64_t in_rows, const int32_t *indices, int64_t m,
+                   int64_t row_bytes, int32_t bytes_per_access, int32_t num_threads, void *stream) {
+  g_last_error.clear();
+  int rc = check_rows_args(out, in, indices, m, row_bytes, bytes_per_access, num_threads);
+  if (rc != SC_OK) return rc;
+  int *err = nullptr;
+  int sms = 0;
+  rc = device_state(&err, &sms);
+  if (rc != SC_OK) return rc;
+  cudaError_t e = scb::launch_gather_rows(out, in, in_rows, indices, m, row_bytes, bytes_per_access,
+                                          num_threads, sms, err, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "gather launch");
+  return SC_OK;
+}
+
+int sc_scatter_add_rows(void *out, int64_t out_rows, const void *in, const int32_t *indices,
+                        int64_t m, int64_t channels, int32_t dtype, int32_t bytes_per_access,
+                        int32_t num_threads, void *stream) {
+  g_last_error.clear();
+  if (dtype != SC_FLOAT32 && !is16(dtype))
+    return fail(SC_RUNTIME, "can't find a sutable scatter: dtype %s", dtype_name(dtype));
+  int rc = check_rows_args(out, in, indices, m, channels * esize(dtype), bytes_per_access, num_threads);
+  if (rc != SC_OK) return rc;
+  int *err = nullptr;
+  int sms = 0;
+  rc = device_state(&err, &sms);
+  if (rc != SC_OK) return rc;
+  cudaError_t e = scb::launch_scatter_add_rows(out, out_rows, in, indices, m, channels, dtype,
+                                               bytes_per_access, num_threads, sms, err,
+                                               static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "scatter launch");
+  return SC_OK;
+}
+
 // ------------------------------------------------------------------ pairs
 int sc_pairs_workspace_size(int64_t n_in, int32_t kv, int32_t subm, int64_t *bytes) {
   if (n_in < 0 || kv < 1 || kv > 32) return fail(SC_INVALID_ARG, "bad n_in / kv");

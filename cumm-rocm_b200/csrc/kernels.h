@@ -149,6 +149,16 @@ struct GemmArgs {
 cudaError_t launch_gemm(const GemmArgs &a, int num_sms, cudaStream_t stream);
 int64_t gemm_workspace_bytes(const GemmArgs &a);
 
+// ------------------------------------------------------------------ gather / scatter
+// out[i] = in[indices[i]] (rows of row_bytes bytes), and
+// out[indices[i]] += in[i] (rows of `channels` elements of dtype 0 / 7 / 12).
+cudaError_t launch_gather_rows(void *out, const void *in, int64_t in_rows, const int32_t *indices,
+                               int64_t m, int64_t row_bytes, int bytes_per_access, int threads,
+                               int num_sms, int *err, cudaStream_t s);
+cudaError_t launch_scatter_add_rows(void *out, int64_t out_rows, const void *in, const int32_t *indices,
+                                    int64_t m, int64_t channels, int dtype, int bytes_per_access,
+                                    int threads, int num_sms, int *err, cudaStream_t s);
+
 // ------------------------------------------------------------------ pair builder
 struct PairBuildArgs {
   const int32_t *coords;

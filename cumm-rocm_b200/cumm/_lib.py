@@ -21,7 +21,7 @@ EXPORTS = (
     "sc_pairs_workspace_size", "sc_build_subm_pairs", "sc_build_conv_outputs",
     "sc_build_conv_pairs", "sc_sort_masks_split", "sc_sort_workspace_size",
     "sc_check_device_error", "sc_last_error", "sc_version", "sc_sort_indices",
-    "sc_conv_wgrad_static_scratch",
+    "sc_conv_wgrad_static_scratch", "sc_gather_rows", "sc_scatter_add_rows",
 )
 
 c_i32, c_i64, c_u32, c_f32, c_vp = (ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32,
@@ -93,6 +93,9 @@ def load() -> ctypes.CDLL:
         lib.sc_sort_workspace_size.argtypes = [c_i64, P(c_i64)]
         lib.sc_check_device_error.argtypes = [c_vp, P(c_i32)]
         lib.sc_sort_indices.argtypes = [c_vp, c_i32, c_i64, c_vp, c_vp, c_vp]
+        lib.sc_gather_rows.argtypes = [c_vp, c_vp, c_i64, c_vp, c_i64, c_i64, c_i32, c_i32, c_vp]
+        lib.sc_scatter_add_rows.argtypes = [c_vp, c_i64, c_vp, c_vp, c_i64, c_i64, c_i32, c_i32,
+                                            c_i32, c_vp]
         lib.sc_last_error.restype = ctypes.c_char_p
         lib.sc_version.restype = ctypes.c_char_p
         for name in EXPORTS:

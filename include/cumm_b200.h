@@ -265,6 +265,30 @@ int sc_sort_workspace_size(int64_t n, int64_t *bytes);
 int sc_sort_indices(const int32_t *indices, int32_t kv, int64_t N, const int32_t *argsort,
                     int32_t *indices_sorted, void *stream);
 
+/*
+ * Standalone row gather and scatter-add.  Replace the reference's
+ * GatherAll.gather / ScatterAll.scatter (cumm/gemm/gather.py:390-620; kernels
+ * GatherKernelV2 and ScatterKernel, gather.py:125-331):
+ *   sc_gather_rows:      out[i, :] = in[indices[i], :] for i < m, rows of
+ *                        row_bytes bytes (any dtype)
+ *   sc_scatter_add_rows: out[indices[i], :] += in[i, :] for i < m, rows of
+ *                        `channels` elements of dtype SC_FLOAT32 (the
+ *                        reference's only scatter dtype), SC_FLOAT16 or
+ *                        SC_BFLOAT16 (added in fp32, rounded once)
+ * bytes_per_access (4, 8 or 16) must divide the row's bytes and the base
+ * addresses; num_threads (64, 128 or 256) is the block size.  As in the
+ * reference, scatter-add reads, adds and writes each row once without
+ * atomics, so the indices of one call must be distinct.  Index -1 gives a zero
+ * row (gather) or skips the row (scatter-add); any other index outside
+ * [0, in_rows) / [0, out_rows) sets the device error word's bad-index bit and
+ * is treated like -1.
+ */
+int sc_gather_rows(void *out, const void *in, int64_t in_rows, const int32_t *indices, int64_t m,
+                   int64_t row_bytes, int32_t bytes_per_access, int32_t num_threads, void *stream);
+int sc_scatter_add_rows(void *out, int64_t out_rows, const void *in, const int32_t *indices,
+                        int64_t m, int64_t channels, int32_t dtype, int32_t bytes_per_access,
+                        int32_t num_threads, void *stream);
+
 /* Device error word of the current device: returns the accumulated error bits
  * (0 = none) after synchronising `stream`, and clears them. */
 int sc_check_device_error(void *stream, int32_t *bits);
