@@ -44,9 +44,31 @@
 // plus kErrWaitTimeout instead of spinning forever.
 #include <cuda.h>
 
+#include <mutex>
+
 #include "kernels.h"
 
 namespace scb {
+
+// Source of the all-zero gathers: kZeroRows 128-byte rows of zeros.  Each
+// gather picks its group of four from a spread of addresses, so the reads do
+// not all land on one L2 slice.
+__device__ __align__(1024) uint8_t g_zero_rows[kZeroRows * 128];
+
+const void *zero_rows_address() {
+  static std::mutex mu;
+  static const void *addr[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (addr[dev] == nullptr) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_zero_rows) != cudaSuccess) return nullptr;
+    addr[dev] = p;
+  }
+  return addr[dev];
+}
+
 namespace {
 
 constexpr int kTileM = 128;
@@ -63,6 +85,11 @@ struct Meta {
 struct KParams {
   CUtensorMap tmap_a;  // gathered rows [a_rows, red] (TMA path)
   CUtensorMap tmap_b;  // B rows [n_total, kv * red] (TMA path)
+  // four rows of zeros with tmap_a's box and swizzle: a gather whose four
+  // rows are all -1 reads these instead (out-of-range gather rows cost the
+  // TMA unit several times an in-range row)
+  CUtensorMap tmap_zero;
+  int zero_ok;
   ConvRowGatherArgs a;
   int64_t num_tiles;
   int cpo;            // chunks per offset (a_row_bytes >= 128), else 0
@@ -82,6 +109,7 @@ struct KParams {
 };
 
 __device__ __forceinline__ void flag_error(int *err, int bits) { atomicOr(err, bits); }
+
 
 // ------------------------------------------------------------------ epilogue helpers
 template <int n, typename TOut>
@@ -522,7 +550,12 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
             flag_error(A.err, kErrBadIndex);
             q = make_int4(-1, -1, -1, -1);
           }
-          tma_gather4(sA + r0 * rb, &P.tmap_a, cb * box, q.x, q.y, q.z, q.w, &full_bar[s]);
+          if (P.zero_ok && (q.x & q.y & q.z & q.w) == -1) {
+            const int z = zero_group(blockIdx.x * 32 + pw * 8 + lane, gchunk);
+            tma_gather4(sA + r0 * rb, &P.tmap_zero, 0, z, z + 1, z + 2, z + 3, &full_bar[s]);
+          }
+          else
+            tma_gather4(sA + r0 * rb, &P.tmap_a, cb * box, q.x, q.y, q.z, q.w, &full_bar[s]);
         }
         ++gchunk;
         if (++stage == static_cast<uint32_t>(S)) {
@@ -806,6 +839,433 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
   }
 }
 
+// ------------------------------------------------------------------ strand kernel
+// Forward / backward-input over 128-byte gathered rows with several
+// independent pipelines ("strands") per SM: two CTAs per SM, each running
+// kStrands strands.  A strand owns kSProd producer warps, its own ring of
+// kSStages stages (128 gathered rows + the weight slab), one MMA warp and a
+// double-buffered TMEM accumulator; the four epilogue warps of the CTA serve
+// both strands.  Measured on B200: one tcgen05.mma stream (one issuing warp)
+// completes an M = 128, K = 16 MMA about every 170 cycles whatever N is, and
+// one producer ring (its warps, stages and barriers) fills ~18-30 bytes per
+// cycle; both rates grow with the number of independent streams on the SM
+// (four MMA warps: ~5450 FLOP/clk/SM at N = 64; four rings of four TMA warps:
+// ~65 B/clk/SM), which the strands provide.  Tiles are dealt round-robin over
+// all strands of the grid.  Every role derives its tiles' masks itself (the
+// tile's mask words OR-ed per 32-row group), and the producers read each
+// gather's four indices straight from the sorted index table, so the strands
+// share no index ring.  Needs indices_sorted (16-byte aligned, M % 4 == 0)
+// and BN <= 64.
+constexpr int kStrands = 2;
+constexpr int kSProd = 4;
+constexpr int kSStages = 2;
+constexpr int kSWarps = kEpiWarps + kStrands * (kSProd + 1);  // 14
+constexpr int kSThreads = kSWarps * 32;
+constexpr int kSBars = 2 * kSStages + 7;  // barriers per strand
+constexpr uint32_t kSTmemCols = 256;      // per CTA: kStrands x 2 buffers x BN (<= 64)
+
+struct TileMasks {
+  uint32_t g[4];    // OR of each 32-row group (unfiltered)
+  uint32_t sub[4];  // mask gating each 32-row group (descriptor tile, filtered, reversed for dgrad)
+  uint32_t tm;      // offsets the tile visits (filtered, reversed for dgrad)
+};
+
+// Lane l loads the mask words of rows q * 32 + l (q < 4) of a 128-row tile.
+__device__ __forceinline__ void load_mask_words(const ConvRowGatherArgs &A, int64_t tile_m, int lane,
+                                                uint32_t (&w)[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int64_t rq = tile_m * kTileM + q * 32 + lane;
+    w[q] = rq < A.M ? (A.mask ? __ldg(A.mask + rq) : 1u) : 0u;
+  }
+}
+
+// Warp-wide: the tile's group ORs, sub-tile masks and tile mask (kernel.py:844-889).
+__device__ __forceinline__ TileMasks reduce_masks(const ConvRowGatherArgs &A, const uint32_t (&w)[4]) {
+  TileMasks t;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint32_t v = w[q];
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, sh);
+    t.g[q] = v;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint32_t sq;
+    if (A.tile_m_desp == 32) sq = t.g[q];
+    else if (A.tile_m_desp == 64) sq = q < 2 ? (t.g[0] | t.g[1]) : (t.g[2] | t.g[3]);
+    else sq = t.g[0] | t.g[1] | t.g[2] | t.g[3];
+    sq &= A.mask_filter;
+    if (A.reverse) sq = __brev(sq) >> (32 - A.kv);
+    t.sub[q] = sq;
+  }
+  uint32_t tm = (t.g[0] | t.g[1] | t.g[2] | t.g[3]) & A.mask_filter;
+  if (A.reverse) tm = __brev(tm) >> (32 - A.kv);
+  t.tm = tm;
+  return t;
+}
+
+template <bool kF8, typename TOut>
+__global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KParams P) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw_u32 = smem_u32(smem_raw);
+  const uint32_t pad = (1024u - (raw_u32 & 1023u)) & 1023u;
+  uint8_t *smem = smem_raw + pad;
+  const uint32_t smem_base = raw_u32 + pad;
+  const ConvRowGatherArgs &A = P.a;
+  constexpr int S = kSStages;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + P.bar_off);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + kStrands * kSBars);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  volatile int *acc_tile = abort_flag + 1;  // [kStrands][2]: tile held by accumulator buffer
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStrands; ++s) {
+      uint64_t *b = bars + s * kSBars;
+      for (int i = 0; i < S; ++i) {
+        mbar_init(&b[i], kSProd);  // full: one arrive.expect_tx per producer warp
+        mbar_init(&b[S + i], 1);   // empty: the MMA commit
+      }
+      mbar_init(&b[2 * S + 0], 1);    // acc_full[0]
+      mbar_init(&b[2 * S + 1], 1);    // acc_full[1]
+      mbar_init(&b[2 * S + 2], 128);  // acc_empty[0]
+      mbar_init(&b[2 * S + 3], 128);  // acc_empty[1]
+      mbar_init(&b[2 * S + 4], 1);    // tile_bar[0]
+      mbar_init(&b[2 * S + 5], 1);    // tile_bar[1]
+      mbar_init(&b[2 * S + 6], 1);    // drain
+    }
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, kSTmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const int64_t nstr = static_cast<int64_t>(gridDim.x) * kStrands;
+
+  if (warp >= kEpiWarps) {
+    const int sw = warp - kEpiWarps;
+    const int s = sw / (kSProd + 1);
+    const int role = sw % (kSProd + 1);  // < kSProd: producer warp, kSProd: MMA warp
+    uint64_t *full = bars + s * kSBars;
+    uint64_t *empty = full + S;
+    uint64_t *acc_full = full + 2 * S;
+    uint64_t *acc_empty = acc_full + 2;
+    uint64_t *tile_bar = acc_full + 4;
+    uint64_t *drain_bar = acc_full + 6;
+    const int64_t first = static_cast<int64_t>(blockIdx.x) * kStrands + s;
+    const uint32_t ring = smem_base + static_cast<uint32_t>(s * S) * P.stage_bytes;
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    if (first < P.num_tiles) load_mask_words(A, first / A.n_tiles, lane, w);
+    if (role < kSProd) {
+      // ---------------------------------------------------------------- producers
+      // Warp pw gathers rows [32 pw, 32 pw + 32) of every chunk: lanes 0-7
+      // each take the four sorted indices of their rows for the chunk's
+      // offset (gated by the row group's sub-tile mask; rows past M read as
+      // -1) and issue one tile::gather4.  The warp whose turn it is adds the
+      // weight slab.  A cursor runs two chunks ahead of the chunk being
+      // issued and loads their indices, so an index load's latency overlaps
+      // the two chunks before it.
+      const int pw = role;
+      const int esz = kF8 ? 1 : 2;
+      const int box = 128 / esz;
+      const uint32_t a_tx = 32u * 128u;
+      const uint32_t b_tx = static_cast<uint32_t>(A.BN) * 128u;
+      const int r0 = pw * 32 + lane * 4;
+      // cursor (warp-uniform): tile, offsets not started yet, current offset / column block
+      int64_t c_tile = first - nstr, c_tile_m = 0;
+      uint32_t c_mm = 0u, c_sub = 0u;
+      int c_k = 0, c_cb = 0, c_n0 = 0;
+      bool c_valid = true;
+      // enters the following tiles until one visits an offset (writing
+      // mask_output for each tile entered)
+      auto next_tile = [&]() {
+        for (;;) {
+          c_tile += nstr;
+          if (c_tile >= P.num_tiles) {
+            c_valid = false;
+            return;
+          }
+          const TileMasks t = reduce_masks(A, w);
+          if (c_tile + nstr < P.num_tiles) load_mask_words(A, (c_tile + nstr) / A.n_tiles, lane, w);
+          c_tile_m = c_tile / A.n_tiles;
+          const int n_tile = static_cast<int>(c_tile % A.n_tiles);
+          c_n0 = n_tile * A.BN;
+          if (pw == 0 && lane == 0 && A.is_fwd && A.mask_out != nullptr && n_tile == 0) {
+            const int nsub = kTileM / A.tile_m_desp;
+            for (int d = 0; d < nsub; ++d) {
+              const int64_t start = c_tile_m * kTileM + d * A.tile_m_desp;
+              if (start >= A.M) break;
+              uint32_t wd;
+              if (nsub == 4) wd = t.g[d];
+              else if (nsub == 2) wd = d == 0 ? (t.g[0] | t.g[1]) : (t.g[2] | t.g[3]);
+              else wd = t.g[0] | t.g[1] | t.g[2] | t.g[3];
+              A.mask_out[start / A.tile_m_desp] = wd & A.mask_filter;
+            }
+          }
+          // rows of lanes 0-7 lie in 32-row group pw
+          c_sub = pw == 0 ? t.sub[0] : pw == 1 ? t.sub[1] : pw == 2 ? t.sub[2] : t.sub[3];
+          if (t.tm != 0u) {
+            c_k = __ffs(t.tm) - 1;
+            c_mm = t.tm & (t.tm - 1u);
+            c_cb = 0;
+            return;
+          }
+        }
+      };
+      auto advance = [&]() {
+        if (++c_cb < P.cpo) return;
+        c_cb = 0;
+        if (c_mm != 0u) {
+          c_k = __ffs(c_mm) - 1;
+          c_mm &= c_mm - 1u;
+          return;
+        }
+        next_tile();
+      };
+      // this lane's four indices of the cursor's chunk (checked when issued,
+      // so the load stays in flight until then)
+      auto load_q = [&]() {
+        int4 q = make_int4(-1, -1, -1, -1);
+        const int64_t rg = c_tile_m * kTileM + r0;
+        if (lane < 8 && rg < A.M && ((c_sub >> c_k) & 1u))
+          q = __ldg(reinterpret_cast<const int4 *>(A.idx_sorted + static_cast<int64_t>(c_k) * A.M + rg));
+        return q;
+      };
+      next_tile();
+      // slots 0 (the chunk to issue) and 1 (the next one)
+      int4 q0 = make_int4(-1, -1, -1, -1), q1 = q0;
+      int k0 = 0, cb0 = 0, n00 = 0, k1 = 0, cb1 = 0, n01 = 0;
+      bool v0 = c_valid, v1 = false;
+      if (c_valid) {
+        q0 = load_q();
+        k0 = c_k; cb0 = c_cb; n00 = c_n0;
+        advance();
+        v1 = c_valid;
+        if (c_valid) {
+          q1 = load_q();
+          k1 = c_k; cb1 = c_cb; n01 = c_n0;
+          advance();
+        }
+      }
+      uint32_t stage = 0, eph = 0, gchunk = 0;
+      while (v0) {
+        // the chunk two ahead: load its indices now
+        int4 q2 = make_int4(-1, -1, -1, -1);
+        int k2 = 0, cb2 = 0, n02 = 0;
+        const bool v2 = c_valid;
+        if (v2) {
+          q2 = load_q();
+          k2 = c_k; cb2 = c_cb; n02 = c_n0;
+          advance();
+        }
+        if (!__all_sync(0xffffffffu, mbar_wait(&empty[stage], eph ^ 1u, abort_flag))) {
+          if (lane == 0) flag_error(A.err, kErrWaitTimeout);
+          break;
+        }
+        const uint32_t sA = ring + stage * P.stage_bytes;
+        if (lane == 0) {
+          if (static_cast<int>(gchunk % kSProd) == pw) {
+            mbar_arrive_expect_tx(&full[stage], a_tx + b_tx);
+            if (P.b_mn) {
+              for (int qq = 0; qq < A.BN / 64; ++qq)
+                tma_load_2d(sA + P.b_off + qq * 8192, &P.tmap_b, k0 * (A.b_off_stride / esz) + n00 + 64 * qq,
+                            cb0 * 64, &full[stage]);
+            } else {
+              tma_load_2d(sA + P.b_off, &P.tmap_b, k0 * (A.b_off_stride / esz) + cb0 * box, n00, &full[stage]);
+            }
+          } else {
+            mbar_arrive_expect_tx(&full[stage], a_tx);
+          }
+        }
+        __syncwarp();
+        if (lane < 8) {
+          if (q0.x < -1 || q0.x >= A.a_rows || q0.y < -1 || q0.y >= A.a_rows || q0.z < -1 || q0.z >= A.a_rows ||
+              q0.w < -1 || q0.w >= A.a_rows) {
+            flag_error(A.err, kErrBadIndex);
+            q0 = make_int4(-1, -1, -1, -1);
+          }
+          if (P.zero_ok && (q0.x & q0.y & q0.z & q0.w) == -1) {
+            const int z = zero_group(blockIdx.x * 64 + warp * 8 + lane, gchunk);
+            tma_gather4(sA + r0 * 128, &P.tmap_zero, 0, z, z + 1, z + 2, z + 3, &full[stage]);
+          }
+          else
+            tma_gather4(sA + r0 * 128, &P.tmap_a, cb0 * box, q0.x, q0.y, q0.z, q0.w, &full[stage]);
+        }
+        ++gchunk;
+        if (++stage == static_cast<uint32_t>(S)) {
+          stage = 0;
+          eph ^= 1u;
+        }
+        q0 = q1; k0 = k1; cb0 = cb1; n00 = n01; v0 = v1;
+        q1 = q2; k1 = k2; cb1 = cb2; n01 = n02; v1 = v2;
+      }
+    } else {
+      // ---------------------------------------------------------------- MMA warp
+      const uint64_t b_kstep = P.b_mn ? 128 : 2;
+      uint32_t stage = 0, fph = 0;
+      bool issued = false, ok = true;
+      int64_t tile = first;
+      for (int it = 0;; ++it, tile += nstr) {
+        const bool have = tile < P.num_tiles;
+        int nch = 0;
+        if (have) {
+          const TileMasks tmk = reduce_masks(A, w);
+          if (tile + nstr < P.num_tiles) load_mask_words(A, (tile + nstr) / A.n_tiles, lane, w);
+          nch = __popc(tmk.tm) * P.cpo;
+        }
+        if (lane == 0) {
+          const int ab = it & 1;
+          const uint32_t aph = (it >> 1) & 1;
+          if (!mbar_wait(&acc_empty[ab], aph ^ 1u, abort_flag)) {
+            flag_error(A.err, kErrWaitTimeout);
+            ok = false;
+          } else {
+            tc_fence_after();
+            // announce the buffer's tile to the epilogue; -1 ends it
+            acc_tile[s * 2 + ab] = have ? static_cast<int>(tile) : -1;
+            mbar_arrive(&tile_bar[ab]);
+            if (have) {
+              const uint32_t d = tmem_base + static_cast<uint32_t>(s * 128 + ab * A.BN);
+              for (int j = 0; j < nch; ++j) {
+                if (!mbar_wait(&full[stage], fph, abort_flag)) {
+                  flag_error(A.err, kErrWaitTimeout);
+                  ok = false;
+                  break;
+                }
+                tc_fence_after();
+                const uint32_t sA = ring + stage * P.stage_bytes;
+                const uint64_t ad = make_sdesc(sA, 16, 1024);
+                const uint64_t bd = P.b_mn ? make_sdesc(sA + P.b_off, 8192, 1024) : make_sdesc(sA + P.b_off, 16, 1024);
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                  if constexpr (kF8)
+                    mma_f8(d, ad + static_cast<uint64_t>(kk * 2), bd + static_cast<uint64_t>(kk) * b_kstep, P.idesc,
+                           (j | kk) != 0 ? 1u : 0u);
+                  else
+                    mma_f16(d, ad + static_cast<uint64_t>(kk * 2), bd + static_cast<uint64_t>(kk) * b_kstep, P.idesc,
+                            (j | kk) != 0 ? 1u : 0u);
+                }
+                issued = true;
+                mma_commit(&empty[stage]);
+                if (++stage == static_cast<uint32_t>(S)) {
+                  stage = 0;
+                  fph ^= 1u;
+                }
+              }
+              if (ok) {
+                if (nch == 0) mbar_arrive(&acc_full[ab]);
+                else mma_commit(&acc_full[ab]);
+              }
+            }
+          }
+        }
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+        if (!ok || !have) break;
+      }
+      if (lane == 0 && issued) {
+        // no tcgen05.mma may be in flight when TMEM is released
+        mma_commit(drain_bar);
+        int never = 0;
+        if (!mbar_wait(drain_bar, 0, reinterpret_cast<volatile int *>(&never))) flag_error(A.err, kErrWaitTimeout);
+      }
+    }
+  } else {
+    // ---------------------------------------------------------------- epilogue (warps 0-3)
+    // Takes the strands' accumulators in turn; thread r owns TMEM lane r (tile row r).
+    const int r = threadIdx.x;
+    const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
+    int its[kStrands];
+    bool done[kStrands];
+    for (int s = 0; s < kStrands; ++s) {
+      its[s] = 0;
+      done[s] = false;
+    }
+    int n_done = 0;
+    bool ok = true;
+    while (n_done < kStrands && ok) {
+      for (int s = 0; s < kStrands && ok; ++s) {
+        if (done[s]) continue;
+        uint64_t *acc_full = bars + s * kSBars + 2 * S;
+        uint64_t *acc_empty = acc_full + 2;
+        uint64_t *tile_bar = acc_full + 4;
+        const int ab = its[s] & 1;
+        const uint32_t aph = (its[s] >> 1) & 1;
+        if (!mbar_wait(&tile_bar[ab], aph, abort_flag)) {
+          flag_error(A.err, kErrWaitTimeout);
+          ok = false;
+          break;
+        }
+        const int tile = acc_tile[s * 2 + ab];
+        if (tile < 0) {
+          done[s] = true;
+          ++n_done;
+          continue;
+        }
+        const int64_t tile_m = tile / A.n_tiles;
+        const int n0 = static_cast<int>(tile % A.n_tiles) * A.BN;
+        const int64_t row_g = tile_m * kTileM + r;
+        const bool valid = row_g < A.M;
+        int sig = valid ? (A.argsort ? __ldg(A.argsort + row_g) : static_cast<int>(row_g)) : -1;
+        if (sig >= A.out_rows) sig = -1;
+        uint32_t km = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int64_t rr = tile_m * kTileM + q * 32 + lane;
+          if (rr < A.M) km |= A.mask ? __ldg(A.mask + rr) : 1u;
+        }
+#pragma unroll
+        for (int sh = 16; sh > 0; sh >>= 1) km |= __shfl_xor_sync(0xffffffffu, km, sh);
+        km &= A.mask_filter;
+        if (!mbar_wait(&acc_full[ab], aph, abort_flag)) {
+          flag_error(A.err, kErrWaitTimeout);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const bool write = valid && sig >= 0 && (A.is_fwd || km != 0);
+        const uint32_t tbase = tmem_base + lane_base + static_cast<uint32_t>(s * 128 + ab * A.BN);
+        for (int cc = 0; cc < A.BN; cc += 16) {
+          float acc[16];
+          if (km != 0) {
+            tmem_ld16(tbase + cc, acc);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[i] = 0.f;
+          }
+          if (write) epilogue_cols<16, TOut>(P, acc, sig, n0 + cc);
+        }
+        tc_fence_before();
+        mbar_arrive(&acc_empty[ab]);
+        ++its[s];
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, kSTmemCols);
+  }
+}
+
+template <bool kF8, typename TOut>
+cudaError_t launch_strands(const KParams &P, int grid, size_t smem, cudaStream_t stream) {
+  void (*kern)(KParams) = conv_strand_kernel<kF8, TOut>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  kern<<<grid, kSThreads, smem, stream>>>(P);
+  return cudaGetLastError();
+}
+
 template <bool kF8, typename TOut>
 cudaError_t launch_typed(const KParams &P, bool tma, bool gather, bool pair, int grid, size_t smem,
                          cudaStream_t stream) {
@@ -872,12 +1332,48 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
       gather = encode_tmap_2d(&P.tmap_a, a.in_dtype, a.a_base, red, static_cast<uint64_t>(a.a_rows),
                               static_cast<uint64_t>(a.a_row_stride), box, 1);
   }
+  // zero rows with the same box and swizzle as the gathered rows
+  P.zero_ok = 0;
+  if (gather) {
+    const void *z = zero_rows_address();
+    const uint32_t zbox = static_cast<uint32_t>(P.row_bytes) / esz;
+    P.zero_ok = z != nullptr && encode_tmap_2d(&P.tmap_zero, a.in_dtype, z, zbox, kZeroRows,
+                                               static_cast<uint64_t>(P.row_bytes), zbox, 1, P.row_bytes)
+                    ? 1 : 0;
+  }
   // the MN-major weight slab is only read by the TMA gather path
   if (a.b_mn && (!gather || a.BN % 64 != 0 || esz != 2)) return cudaErrorInvalidConfiguration;
   const uint32_t a_bytes = kTileM * static_cast<uint32_t>(P.row_bytes);
   const uint32_t b_bytes = static_cast<uint32_t>(a.BN) * P.row_bytes;
   P.stage_bytes = a_bytes + b_bytes;
   P.b_off = a_bytes;
+  // Strands (two independent pipelines per CTA, two CTAs per SM) on the TMA
+  // gather path of 128-byte rows with the sorted index table and BN <= 64
+  // (TMEM: 2 strands x 2 buffers x BN columns per CTA).
+  if (gather && P.row_bytes == 128 && P.bulk_idx && a.BN <= 64) {
+    if (P.num_tiles == 0) return cudaSuccess;
+    P.stages = kSStages;
+    P.tmem_cols = kSTmemCols;
+    P.bar_off = P.stage_bytes * kStrands * kSStages;
+    const size_t smem = 1024 + P.bar_off + 512;
+    const int64_t ctas = (P.num_tiles + kStrands - 1) / kStrands;
+    const int grid = static_cast<int>(ctas < 2 * num_sms ? ctas : 2 * num_sms);
+    if (a.in_dtype == 14) {
+      P.idesc = make_idesc(128, a.BN, 0u, false, false);
+      switch (a.out_dtype) {
+        case 0: return launch_strands<true, float>(P, grid, smem, stream);
+        case 7: return launch_strands<true, __half>(P, grid, smem, stream);
+        default: return launch_strands<true, __nv_bfloat16>(P, grid, smem, stream);
+      }
+    }
+    P.idesc = make_idesc(128, a.BN, a.in_dtype == 12 ? 1u : 0u, false, a.b_mn != 0);
+    switch (a.out_dtype) {
+      case 0: return launch_strands<false, float>(P, grid, smem, stream);
+      case 7: return launch_strands<false, __half>(P, grid, smem, stream);
+      case 12: return launch_strands<false, __nv_bfloat16>(P, grid, smem, stream);
+      default: return cudaErrorInvalidValue;
+    }
+  }
   P.idx_buf_bytes = ((static_cast<uint32_t>(a.kv) * kTileM * 4 + sizeof(Meta)) + 127u) & ~127u;
   uint32_t cols = 32;
   while (cols < static_cast<uint32_t>(2 * a.BN)) cols <<= 1;

@@ -66,6 +66,8 @@ struct WMeta {
 struct WParams {
   CUtensorMap tmap_in;    // input rows [in_rows, C], one-row boxes (gather path)
   CUtensorMap tmap_dout;  // dOut rows [dout_rows, K], one-row boxes (gather path)
+  CUtensorMap tmap_zero;  // four zero rows: gathers whose rows are all -1 read these
+  int zero_ok;
   ConvWgradArgs a;
   int n_chunks;        // ceil(N / 64)
   int chunks_per_cta;
@@ -376,8 +378,13 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
         if (lane < kGpw * n_b_atoms) {
           const int na = lane / kGpw;
           const int4 q = *reinterpret_cast<const int4 *>(sig_tab + rq);
-          tma_gather4(smem_base + P.bbuf_off + bb * (n_b_atoms * 8192u) + na * 8192u + rq * 128,
-                      &P.tmap_dout, na * 64, q.x, q.y, q.z, q.w, &bfull[bb]);
+          const uint32_t dst = smem_base + P.bbuf_off + bb * (n_b_atoms * 8192u) + na * 8192u + rq * 128;
+          if (P.zero_ok && (q.x & q.y & q.z & q.w) == -1) {
+            const int z = zero_group(blockIdx.x * 64 + pw * 8 + lane, static_cast<uint32_t>(it));
+            tma_gather4(dst, &P.tmap_zero, 0, z, z + 1, z + 2, z + 3, &bfull[bb]);
+          }
+          else
+            tma_gather4(dst, &P.tmap_dout, na * 64, q.x, q.y, q.z, q.w, &bfull[bb]);
         }
         if (++bb == P.n_bbuf) {
           bb = 0;
@@ -406,8 +413,13 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
           int4 q = make_int4(-1, -1, -1, -1);
           if (a < P.n_atoms && k < A.kv)
             q = *reinterpret_cast<const int4 *>(tab + (k - k_lo) * kRows + rq);
-          tma_gather4(smem_base + s * P.stage_bytes + (lane / kGpw) * 8192u + rq * 128, &P.tmap_in,
-                      (a % P.cpa) * 64, q.x, q.y, q.z, q.w, &full_bar[s]);
+          const uint32_t dst = smem_base + s * P.stage_bytes + (lane / kGpw) * 8192u + rq * 128;
+          if (P.zero_ok && (q.x & q.y & q.z & q.w) == -1) {
+            const int z = zero_group(blockIdx.x * 64 + pw * 8 + lane, static_cast<uint32_t>(stage + it));
+            tma_gather4(dst, &P.tmap_zero, 0, z, z + 1, z + 2, z + 3, &full_bar[s]);
+          }
+          else
+            tma_gather4(dst, &P.tmap_in, (a % P.cpa) * 64, q.x, q.y, q.z, q.w, &full_bar[s]);
         }
       }
       if (!ok) break;
@@ -698,6 +710,11 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t 
                             static_cast<uint64_t>(a.in_rows), static_cast<uint64_t>(a.in_ld) * 2, 64, 1) &&
              encode_tmap_2d(&P.tmap_dout, a.in_dtype, a.dout, static_cast<uint64_t>(a.K),
                             static_cast<uint64_t>(a.dout_rows), static_cast<uint64_t>(a.dout_ld) * 2, 64, 1);
+  P.zero_ok = 0;
+  if (gather) {
+    const void *z = zero_rows_address();
+    P.zero_ok = z != nullptr && encode_tmap_2d(&P.tmap_zero, a.in_dtype, z, 64, kZeroRows, 128, 64, 1) ? 1 : 0;
+  }
   const uint32_t a_bytes = 2 * 8192;
   const uint32_t b_bytes = static_cast<uint32_t>(P.n_mma / 64) * 8192;
   P.stage_bytes = gather ? a_bytes : a_bytes + b_bytes;

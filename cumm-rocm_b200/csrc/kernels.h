@@ -15,6 +15,17 @@ bool encode_tmap_2d(void *out_map, int dtype, const void *base, uint64_t inner, 
                     uint64_t row_stride_bytes, uint32_t box_inner, uint32_t box_outer,
                     int swizzle_bytes = 128);
 
+// Device address (current device) of four 128-byte rows of zeros that
+// tile::gather4 reads in place of a group of four absent rows (index -1):
+// out-of-range gather rows cost the TMA unit several times an in-range row.
+// Looked up once per device; nullptr if the lookup fails.
+const void *zero_rows_address();
+constexpr int kZeroRows = 512;
+// First row of a group of four zero rows for gather `c` of thread slot `t`.
+__device__ __forceinline__ int zero_group(uint32_t t, uint32_t c) {
+  return static_cast<int>(((t * 37u + c * 101u) & (kZeroRows / 4 - 1)) * 4u);
+}
+
 // ------------------------------------------------------------------ conv fwd / dgrad (tcgen05)
 // Row-gather implicit GEMM: for every 128-row tile of the sorted row order,
 //   out[sigma(r), n] = epi( sum_{k in tile mask} sum_c A[idx[k][sigma(r)], c] * B[n, k, c] )

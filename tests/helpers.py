@@ -36,8 +36,11 @@ def i32(x):
 
 def conv(op, desp, inp, weight, out, indices, mask, argsort, mask_output=None, mask_filter=0xffffffff,
          reverse_mask=False, mask_width=-1, alpha=1.0, beta=0.0, bias=None, scale=None,
-         output_add=None, act_type=0, act_alpha=0.0, sync_check=True):
-    """inp / weight / out are torch tensors (already on the GPU)."""
+         output_add=None, act_type=0, act_alpha=0.0, sync_check=True, sorted_indices=False, tile_n=0):
+    """inp / weight / out are torch tensors (already on the GPU).  With
+    sorted_indices the index table permuted into argsort order is passed as
+    well (ConvParams.indices_sorted), which selects the kernels that read it
+    (the strand kernel for 128-byte rows, N % 4 == 0 and tile_n <= 64)."""
     p = ConvParams(3, op)
     p.conv_algo_desp = desp
     p.input = tv.Tensor(inp, desp.dtype_input)
@@ -46,6 +49,10 @@ def conv(op, desp, inp, weight, out, indices, mask, argsort, mask_output=None, m
     p.indices = i32(indices)
     p.mask = u32(mask)
     p.mask_argsort = i32(argsort)
+    if sorted_indices:
+        p.indices_sorted = i32(np.ascontiguousarray(np.asarray(indices)[:, np.asarray(argsort)]))
+    if tile_n:
+        p.tile_n = tile_n
     if mask_output is not None:
         p.mask_output = mask_output
     p.mask_filter = mask_filter

@@ -36,7 +36,8 @@ def _assert_close(y, ref, tol):
 @pytest.mark.parametrize("n,grid,C,K", [(3000, 24, 64, 64), (1000, 16, 32, 48), (777, 16, 16, 16),
                                         (2000, 20, 128, 128), (500, 12, 96, 32)])
 @pytest.mark.parametrize("tile_m", [128, 32])
-def test_fwd_tcgen05(dt, n, grid, C, K, tile_m):
+@pytest.mark.parametrize("sorted_idx", [False, True])
+def test_fwd_tcgen05(dt, n, grid, C, K, tile_m, sorted_idx):
     coords, pf, pb, m = _subm(n, grid, n)
     rng = np.random.default_rng(1)
     x = rng.standard_normal((n, C)).astype(np.float32)
@@ -46,15 +47,17 @@ def test_fwd_tcgen05(dt, n, grid, C, K, tile_m):
     out = torch.zeros((n, K), dtype=TORCH[dt], device="cuda")
     mo = tv.zeros([(n + tile_m - 1) // tile_m], tv.uint32, 0)
     conv(ConvOpType.kForward, find_desp(ConvOpType.kForward, "Tcgen05", dt, dt, dt, tile_m),
-         xt, wt, out, pf, ms, order, mask_output=mo)
+         xt, wt, out, pf, ms, order, mask_output=mo, sorted_indices=sorted_idx)
     ref, mo_ref = co.conv_fwd_masked(to64(xt), to64(wt), pf, ms, order, tile_m)
     _assert_close(to64(out), ref, TOL_16)
     assert np.array_equal(mo.numpy(), mo_ref)
 
 
 @pytest.mark.parametrize("dt", [tv.bfloat16, tv.float16])
-@pytest.mark.parametrize("n,grid,C,K", [(3000, 24, 64, 64), (1000, 16, 48, 32), (600, 12, 16, 16)])
-def test_dgrad_tcgen05(dt, n, grid, C, K):
+@pytest.mark.parametrize("n,grid,C,K", [(3000, 24, 64, 64), (1000, 16, 48, 32), (600, 12, 16, 16),
+                                        (1500, 16, 64, 128), (1200, 16, 32, 64)])
+@pytest.mark.parametrize("sorted_idx", [False, True])
+def test_dgrad_tcgen05(dt, n, grid, C, K, sorted_idx):
     coords, pf, pb, m = _subm(n, grid, n + 1)
     rng = np.random.default_rng(3)
     dy = rng.standard_normal((n, K)).astype(np.float32)
@@ -64,7 +67,7 @@ def test_dgrad_tcgen05(dt, n, grid, C, K):
     din = torch.zeros((n, C), dtype=TORCH[dt], device="cuda")
     conv(ConvOpType.kBackwardInput,
          find_desp(ConvOpType.kBackwardInput, "Tcgen05", dt, dt, dt, 128),
-         din, wt, dyt, pb, ms, order, reverse_mask=True)
+         din, wt, dyt, pb, ms, order, reverse_mask=True, sorted_indices=sorted_idx)
     ref = co.conv_dgrad_masked(to64(dyt), to64(wt), pb, ms, order, 128, reverse_mask=True)
     _assert_close(to64(din), ref, TOL_16)
 
@@ -436,3 +439,74 @@ def test_sorted_index_table_identical(n):
     # (run-to-run) summation order
     nr = (torch.linalg.norm(outs[0][2] - outs[1][2]) / torch.linalg.norm(outs[0][2])).item()
     assert nr < 1e-6, nr
+
+
+@pytest.mark.parametrize("n,grid,C,K,tile_n,tile_m", [
+    (4000, 24, 64, 64, 0, 128), (4000, 24, 64, 64, 32, 64), (4000, 24, 64, 64, 16, 32),
+    (2000, 20, 128, 64, 0, 128), (2000, 20, 64, 128, 64, 128), (2000, 20, 128, 128, 64, 32),
+    (4, 8, 64, 64, 0, 128), (132, 10, 64, 64, 0, 128)])
+def test_strand_kernel_shapes(n, grid, C, K, tile_n, tile_m):
+    """Forward and backward-input through the strand kernel (sorted index
+    table, 128-byte rows, column tiles <= 64): several chunks per offset
+    (C = 128), several column tiles (K = 128 with tile_n 64), sub-tile masks
+    (tile_shape[0] 32 / 64) with mask_output, a split mask_filter with beta = 1
+    on the second launch, and tiny and ragged N, against the FP64 oracle."""
+    coords, pf, pb, m = _subm(n, grid, n + 7)
+    rng = np.random.default_rng(n)
+    xt = dev(rng.standard_normal((n, C)).astype(np.float32), torch.bfloat16)
+    wt = dev(vg.kaiming_uniform(K, 27, C, n), torch.bfloat16)
+    dyt = dev(rng.standard_normal((n, K)).astype(np.float32), torch.bfloat16)
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.float32, tile_m)
+    out = torch.zeros((n, K), dtype=torch.float32, device="cuda")
+    mo = tv.zeros([(n + tile_m - 1) // tile_m], tv.uint32, 0)
+    conv(ConvOpType.kForward, desp, xt, wt, out, pf, ms, order, mask_output=mo, sorted_indices=True,
+         tile_n=tile_n)
+    ref, mo_ref = co.conv_fwd_masked(to64(xt), to64(wt), pf, ms, order, tile_m)
+    _assert_close(to64(out), ref, TOL_16)
+    assert np.array_equal(mo.numpy(), mo_ref)
+    # MaskSplitImplicitGemm form: two launches over the split masks, beta 1 on the second
+    out2 = torch.zeros((n, K), dtype=torch.float32, device="cuda")
+    for j, sm in enumerate(po.split_masks(27, 2)):
+        msj, oj = po.sort_by_key_split(m, sm)
+        conv(ConvOpType.kForward, desp, xt, wt, out2, pf, msj, oj, mask_filter=sm, beta=1.0 if j else 0.0,
+             sorted_indices=True, tile_n=tile_n)
+    _assert_close(to64(out2), ref, TOL_16)
+    dd = find_desp(ConvOpType.kBackwardInput, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, tile_m)
+    din = torch.zeros((n, C), dtype=torch.bfloat16, device="cuda")
+    conv(ConvOpType.kBackwardInput, dd, din, wt, dyt, pb, ms, order, reverse_mask=True, sorted_indices=True,
+         tile_n=tile_n if C % max(tile_n, 1) == 0 else 0)
+    _assert_close(to64(din), co.conv_dgrad_masked(to64(dyt), to64(wt), pb, ms, order, tile_m, reverse_mask=True),
+                  TOL_16)
+
+
+def test_strand_kernel_fp8_and_bad_index():
+    """E4M3 operands with 128-byte rows (C = 128) and the scale epilogue on the
+    strand kernel, and a bad index in the sorted table reported as a device
+    error instead of being gathered."""
+    n, grid, C, K = 2000, 20, 128, 64
+    coords, pf, pb, m = _subm(n, grid, 31)
+    rng = np.random.default_rng(31)
+    x = rng.standard_normal((n, C)).astype(np.float32)
+    w = vg.kaiming_uniform(K, 27, C, 31)
+    sx = np.abs(x).max() / 448.0
+    sw = np.abs(w).reshape(K, -1).max(1) / 448.0
+    xq = dev(x / sx, torch.float8_e4m3fn)
+    wq = dev(w / sw[:, None, None], torch.float8_e4m3fn)
+    scale = dev((sx * sw).astype(np.float32))
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    out = torch.zeros((n, K), dtype=torch.bfloat16, device="cuda")
+    desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.float_e4m3, tv.float_e4m3, tv.bfloat16, 128)
+    conv(ConvOpType.kForward, desp, xq, wq, out, pf, ms, order, scale=scale, sorted_indices=True)
+    ref, _ = co.conv_fwd_masked(to64(xq), to64(wq), pf, ms, order, 128, scale=(sx * sw).astype(np.float64))
+    _assert_close(to64(out), ref, TOL_16)
+    bad = pf.copy()
+    r = int(order[5])
+    k = int(np.nonzero(pf[:, r] >= 0)[0][0])
+    bad[k, r] = n + 50
+    xb = dev(rng.standard_normal((n, 64)).astype(np.float32), torch.bfloat16)
+    wb = dev(vg.kaiming_uniform(64, 27, 64, 1), torch.bfloat16)
+    ob = torch.zeros((n, 64), dtype=torch.bfloat16, device="cuda")
+    db = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 128)
+    with pytest.raises(RuntimeError, match="device error"):
+        conv(ConvOpType.kForward, db, xb, wb, ob, bad, ms, order, sorted_indices=True)
