@@ -17,6 +17,16 @@ fp32 accumulation: forward + backward-input + backward-weight).
 * ``cpu_baseline`` / ``--impl reference``: the reference's own CPU algorithm
   for this path (numpy gather-GEMM-scatter, cumm/conv/main_real_spconv.py:309-403)
   restated in oracle/conv_oracle.py, fp32, BLAS on all host cores.
+* ``batched`` (N = 1): 64 LiDAR-like clouds (lognormal voxel counts, median
+  40k, sigma 0.8, clipped to [5k, 300k]) through the same subm 3x3x3 C = K = 64
+  bf16 layer: one grouped persistent launch replayed from a CUDA graph vs 64
+  sequential one-cloud calls (the reference's plain path), with and without
+  the pair build; the grouped result is checked against the FP64 oracle.
+* ``served`` (N = 1): the 10-layer sparse encoder served at 800 req/s
+  (Poisson arrivals, clouds of 10k-400k voxels) in plain one-request-at-a-time
+  mode and with continuous batching: p50 / p99 latency and voxels/s of both;
+  every layer of one request is checked against the FP64 oracle, and that
+  request's result alone equals its result inside the mix.
 Multi-GPU: independent clouds per rank (weak scaling, no collective on the
 data path).
 """
@@ -92,6 +102,32 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sms)) if sms else None,
                 "sm_max_mhz": float(max(maxs)) if maxs else None,
                 "samples": len(sms), "reasons": sorted(reasons)}
+
+
+KERNEL_SOURCE = {"conv_fwd_rowgather": "conv_rowgather.cu", "conv_dgrad_rowgather": "conv_rowgather.cu",
+                 "conv_wgrad": "conv_wgrad.cu"}
+
+
+def source_sha(kernel: str) -> str:
+    import hashlib
+    src = ROOT / "cumm-rocm_b200" / "csrc" / KERNEL_SOURCE[kernel]
+    return hashlib.sha256(src.read_bytes()).hexdigest()[:16]
+
+
+def recorded_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the ncu capture recorded in
+    profiles/traffic.json, used only when the capture was taken of the
+    current kernel source (its sha256 prefix is stored with the bytes);
+    otherwise None and a note saying the capture is stale."""
+    tfile = ROOT / "profiles" / "traffic.json"
+    if not tfile.exists():
+        return None, "no ncu capture recorded"
+    rec = json.loads(tfile.read_text()).get(kernel)
+    if not isinstance(rec, dict):
+        return None, "no ncu capture recorded for this kernel"
+    if rec.get("source_sha") != source_sha(kernel):
+        return None, f"recorded capture ({rec.get('bytes')} B) was taken of an older kernel source"
+    return rec["bytes"], f"ncu capture of the current source ({rec.get('capture', '')})"
 
 
 def max_over_ranks(x: float, dist, device) -> float:
@@ -178,6 +214,82 @@ def run_reference(args, rank, world):
     }
     print(json.dumps(line), flush=True)
     return line
+
+
+def run_batched(reps: int = 3) -> dict:
+    """Config 4: grouped + graph-replayed forward over 64 clouds vs sequential
+    per-cloud calls (cumm.batch)."""
+    from cumm import batch
+    res = batch.main(reps=reps, verbose=False, keep=True)
+    return res
+
+
+def run_served(rate: float = 800.0, n_req: int = 160, seed: int = 0) -> dict:
+    """Config 5: one point of the serving sweep, plain vs continuous, on the
+    same seeded request stream (cumm.serve)."""
+    import torch
+
+    from cumm import serve as sv
+    from cumm import voxelgen as vg
+    enc = sv.SparseEncoder(vg.KITTI_SHAPE, seed=seed)
+    pool = sv.make_pool(k=16, seed=seed)
+    sv.serve(enc, sv.make_requests(8, 1000.0, seed + 99, pool=pool), continuous=False)
+    for _ in range(2):
+        sv.serve(enc, sv.make_requests(96, 5000.0, seed + 98, pool=pool), continuous=True)
+    out = {"rate_req_s": rate, "requests": n_req,
+           "encoder": "subm16x2,down32,subm32,down64,subm64x2,down128,subm128x2 (ReLU), bf16"}
+    for continuous in (False, True):
+        reqs = sv.make_requests(n_req, rate, seed + int(rate), pool=pool)
+        st = sv.serve(enc, reqs, continuous=continuous, keep_outputs=continuous)
+        out["continuous" if continuous else "plain"] = {
+            k: st[k] for k in ("p50_ms", "p99_ms", "voxels_per_s", "makespan_s", "passes", "mean_batch")}
+        if continuous:
+            mixed = reqs
+    out["voxels_per_s_ratio"] = out["continuous"]["voxels_per_s"] / out["plain"]["voxels_per_s"]
+    # one request alone vs inside the mix (the check below compares them)
+    small = min(mixed, key=lambda r: r.n)
+    alone = sv.Request(small.rid, 0.0, small.coords, small.feats)
+    sv.serve(enc, [alone], continuous=False, keep_outputs=True)
+    torch.cuda.synchronize()
+    out["_check"] = (enc, small, alone)
+    return out
+
+
+def check_batched_and_served(batched: dict, served: dict) -> None:
+    """The checker: FP64 oracle errors of the batched result (smallest cloud)
+    and of every encoder layer of one served request, and alone-vs-mix
+    identity of that request.  Fills the dicts' "max_norm_rel_vs_fp64" keys."""
+    import torch
+
+    from cumm import voxelgen as vg
+    from oracle import conv_oracle as co
+    from oracle import pairs_oracle as po
+
+    def to64(t):
+        return t.float().cpu().numpy().astype(np.float64)
+
+    if batched is not None:
+        st = batched.pop("state")
+        i = int(np.argmin([c.shape[0] for c in st["coords"]]))
+        c = st["coords"][i].cpu().numpy()
+        pf, _, _ = po.subm_pairs(c, vg.KITTI_SHAPE)
+        ref = co.fwd_gather_gemm_scatter(to64(st["feats"][i]), to64(st["weight"]), pf)
+        nr, mr, _ = co.rel_err(to64(st["outputs"][i]), ref)
+        batched["checked_cloud_voxels"] = int(c.shape[0])
+        batched["max_norm_rel_vs_fp64"] = float(nr)
+    if served is not None:
+        enc, mixed, alone = served.pop("_check")
+        served["alone_equals_mix"] = bool(torch.equal(mixed.out, alone.out) and
+                                          torch.equal(mixed.out_coords, alone.out_coords))
+        rec = []
+        enc.forward(alone.coords.cuda(), alone.feats.cuda(), record=rec)
+        torch.cuda.synchronize()
+        worst = 0.0
+        for li, (x, pt, y) in enumerate(rec):
+            ref = np.maximum(co.fwd_gather_gemm_scatter(to64(x), to64(enc.wb[li]), pt.pairs_fwd.cpu().numpy()), 0.0)
+            worst = max(worst, co.rel_err(to64(y), ref)[0])
+        served["checked_request_voxels"] = int(alone.n)
+        served["max_norm_rel_vs_fp64"] = float(worst)
 
 
 def run_b200(args, rank, world, dist):
@@ -408,10 +520,7 @@ def run_b200(args, rank, world, dist):
     dom = int(np.argmax(ms_op))
     peak_tf, peak_bw, peak_kind = _peaks()
     achieved = flops_op / (ms_op[dom] * 1e-3) / 1e12
-    traffic = None
-    tfile = ROOT / "profiles" / "traffic.json"
-    if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(names[dom])
+    traffic, traffic_note = recorded_traffic(names[dom])
     # algorithmic bytes of one op: features in + out (or dOut + In for wgrad),
     # weights, the [kv, N] index table, masks and argsort
     alg_bytes = (N_VOX * C * 2 + N_VOX * K * 2 + KV * C * K * (4 if dom == 2 else 2)
@@ -419,12 +528,20 @@ def run_b200(args, rank, world, dist):
     hbm_achieved = alg_bytes / (ms_op[dom] * 1e-3) / 1e9
     roofline = {"bound": "tensor", "kernel": names[dom], "achieved": achieved, "peak": peak_tf,
                 "unit": "TFLOP/s", "frac": achieved / peak_tf, "peak_kind": peak_kind,
-                "traffic": traffic,
+                "traffic": traffic, "traffic_note": traffic_note,
                 "hbm": {"algorithmic_bytes": alg_bytes, "achieved_gbs": hbm_achieved,
                         "peak_gbs": peak_bw, "frac": hbm_achieved / peak_bw}}
 
+    # ---------------------------------------------------------------- batched / served forms (N = 1)
+    batched = served = None
+    if world == 1 and not args.no_batched:
+        batched = run_batched()
+    if world == 1 and not args.no_served:
+        served = run_served()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        check_batched_and_served(batched, served)
         _, pf, pb, _, xc, dyc, wc = _cpu_data(0)
         t0 = time.perf_counter()
         cpu_reference_step(xc, wc, dyc, pf, pb)
@@ -434,6 +551,12 @@ def run_b200(args, rank, world, dist):
                "cores": os.cpu_count(), "kind": "port",
                "sample": "one full step (fwd+dgrad+wgrad) of the same 200k-voxel layer, numpy "
                          "fp32 gather-GEMM-scatter, BLAS on all host cores"}
+
+    # objects kept only for the checker
+    if batched is not None:
+        batched.pop("state", None)
+    if served is not None:
+        served.pop("_check", None)
 
     if rank == 0:
         line = {
@@ -453,6 +576,8 @@ def run_b200(args, rank, world, dist):
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "steps": n_e2e, "pipelined_streams": 3, "buffer_sets": NBUF},
             "cpu_baseline": cpu,
+            "batched": batched,
+            "served": served,
             "gpu_launches": 5 * args.steps,
             "clocks": clocks,
         }
@@ -467,6 +592,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end loop (profiling)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-cloud grouped vs sequential run")
+    ap.add_argument("--no-served", action="store_true", help="skip the serving point (800 req/s)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -121,7 +121,11 @@ def lognormal_counts(n: int, median: float, sigma: float, lo: int, hi: int, seed
 
 
 def main(n_clouds: int = 64, median: int = 40_000, sigma: float = 0.8, C: int = 64, K: int = 64,
-         seed: int = 0, reps: int = 5) -> dict:
+         seed: int = 0, reps: int = 5, verbose: bool = True, keep: bool = False) -> dict:
+    """Config-4 comparison: grouped + graph-replayed vs sequential per-cloud
+    calls.  Returns the result dict (printed as one JSON line when verbose);
+    with keep=True it also holds "state": the clouds, features, weight and the
+    grouped output split per cloud, for an outside check of the numbers."""
     import json
 
     from cumm import voxelgen as vg
@@ -202,7 +206,10 @@ def main(n_clouds: int = 64, median: int = 40_000, sigma: float = 0.8, C: int = 
                       "grouped_tflops": flops / (ms_grp_conv * 1e-3) / 1e12},
         "max_norm_rel_grouped_vs_sequential": worst,
     }
-    print(json.dumps(res), flush=True)
+    if verbose:
+        print(json.dumps(res), flush=True)
+    if keep:
+        res["state"] = {"coords": coords, "feats": feats, "weight": w, "outputs": grouped.split(y)}
     return res
 
 
