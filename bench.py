@@ -24,7 +24,8 @@ fp32 accumulation: forward + backward-input + backward-weight).
   the pair build; the grouped result is checked against the FP64 oracle.
 * ``served`` (N = 1): the 10-layer sparse encoder served at 800 req/s
   (Poisson arrivals, clouds of 10k-400k voxels) in plain one-request-at-a-time
-  mode and with continuous batching: p50 / p99 latency and voxels/s of both;
+  mode and with continuous batching: p50 / p99 latency and voxels/s of both,
+  and both modes' capacity (``saturated``: every request arriving at once);
   every layer of one request is checked against the FP64 oracle, and that
   request's result alone equals its result inside the mix.
 Multi-GPU: independent clouds per rank (weak scaling, no collective on the
@@ -233,9 +234,12 @@ def run_served(rate: float = 800.0, n_req: int = 160, seed: int = 0) -> dict:
     from cumm import voxelgen as vg
     enc = sv.SparseEncoder(vg.KITTI_SHAPE, seed=seed)
     pool = sv.make_pool(k=16, seed=seed)
+    # warm-up: kernels loaded, and the caching allocator of every pass stream
+    # holds the buffers of the largest passes (growing it synchronizes)
     sv.serve(enc, sv.make_requests(8, 1000.0, seed + 99, pool=pool), continuous=False)
     for _ in range(2):
-        sv.serve(enc, sv.make_requests(96, 5000.0, seed + 98, pool=pool), continuous=True)
+        sv.serve(enc, sv.make_requests(n_req, 1e7, seed + 98, pool=pool), continuous=True)
+        sv.serve(enc, sv.make_requests(96, 5000.0, seed + 97, pool=pool), continuous=True)
     out = {"rate_req_s": rate, "requests": n_req,
            "encoder": "subm16x2,down32,subm32,down64,subm64x2,down128,subm128x2 (ReLU), bf16"}
     for continuous in (False, True):
@@ -246,12 +250,98 @@ def run_served(rate: float = 800.0, n_req: int = 160, seed: int = 0) -> dict:
         if continuous:
             mixed = reqs
     out["voxels_per_s_ratio"] = out["continuous"]["voxels_per_s"] / out["plain"]["voxels_per_s"]
+    # capacity: the same number of requests all arriving at once, so neither
+    # mode waits for arrivals (at 800 req/s continuous batching keeps pace with
+    # the arrivals and its voxels/s is the offered load)
+    sat = {}
+    for continuous in (False, True):
+        reqs = sv.make_requests(n_req, 1e7, seed + 7, pool=pool)
+        st = sv.serve(enc, reqs, continuous=continuous)
+        sat["continuous" if continuous else "plain"] = {
+            k: st[k] for k in ("p50_ms", "p99_ms", "voxels_per_s", "makespan_s", "passes", "mean_batch")}
+    sat["voxels_per_s_ratio"] = sat["continuous"]["voxels_per_s"] / sat["plain"]["voxels_per_s"]
+    out["saturated"] = sat
     # one request alone vs inside the mix (the check below compares them)
     small = min(mixed, key=lambda r: r.n)
     alone = sv.Request(small.rid, 0.0, small.coords, small.feats)
     sv.serve(enc, [alone], continuous=False, keep_outputs=True)
     torch.cuda.synchronize()
     out["_check"] = (enc, small, alone)
+    return out
+
+
+def run_aux(peak_tf: float, peak_bw: float) -> dict:
+    """Kernels beside the conv step, timed with CUDA events (L2-resident
+    inputs unless stated): the dense tcgen05 matmul2 on an 8192^3 bf16 GEMM
+    (cuBLAS through torch.matmul on the same shape for context), a tall-K
+    ShuffleAB GEMM (200k gathered rows, the native backward-weight form), and
+    the standalone gather / scatter-add on 128-byte rows (4M rows: 512 MB,
+    HBM-bound)."""
+    import torch
+
+    from cumm import tensorview as tv
+    from cumm.gemm.gather import GatherAll, ScatterAll
+    from cumm.gemm.main import GemmMainUnitTest, get_all_algo_desp
+    from cumm.tensorview.gemm import GemmParams, ShuffleStrideType
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def desp(st, ta, tb, dc):
+        for d in get_all_algo_desp():
+            if (d.algo == "Tcgen05" and d.dtype_a == tv.bfloat16 and d.dtype_c == dc and d.trans_a == ta
+                    and d.trans_b == tb and d.shuffle_type == st):
+                return d
+        raise KeyError(st)
+
+    out = {}
+    g = GemmMainUnitTest()
+    n = 8192
+    a = torch.randn(n, n, device="cuda").bfloat16()
+    b = torch.randn(n, n, device="cuda").bfloat16()
+    c = torch.empty(n, n, device="cuda", dtype=torch.bfloat16)
+    p = GemmParams()
+    p.algo_desp = desp(ShuffleStrideType.kNoShuffle, False, False, tv.bfloat16)
+    p.a, p.b, p.c = tv.Tensor(a), tv.Tensor(b), tv.Tensor(c)
+    ms = timed(lambda: g.matmul2(p), 10)
+    ms_cublas = timed(lambda: torch.matmul(a, b, out=c), 10)
+    fl = 2.0 * n ** 3
+    out["dense_gemm_8192_bf16"] = {"ms": ms, "tflops": fl / ms / 1e9, "frac_of_peak": fl / ms / 1e9 / peak_tf,
+                                   "cublas_ms": ms_cublas, "cublas_tflops": fl / ms_cublas / 1e9}
+    rows, ko, ci = 200_000, 64, 128
+    do = torch.randn(rows, ko, device="cuda").bfloat16()
+    xi = torch.randn(rows, ci, device="cuda").bfloat16()
+    perm = torch.randperm(rows, device="cuda").int()
+    c2 = torch.empty(ko, ci, device="cuda")
+    p2 = GemmParams()
+    p2.algo_desp = desp(ShuffleStrideType.kShuffleAB, True, False, tv.float32)
+    p2.a, p2.b, p2.c = tv.Tensor(do), tv.Tensor(xi), tv.Tensor(c2)
+    p2.a_inds, p2.b_inds = tv.Tensor(perm), tv.Tensor(torch.randperm(rows, device="cuda").int())
+    ms2 = timed(lambda: g.matmul2(p2), 20)
+    fl2 = 2.0 * rows * ko * ci
+    out["shuffle_ab_tallk_200k_64x128_bf16"] = {"ms": ms2, "tflops": fl2 / ms2 / 1e9,
+                                                 "frac_of_peak": fl2 / ms2 / 1e9 / peak_tf}
+    m = 4_000_000
+    src = torch.randn(m, 64, device="cuda").bfloat16()
+    dst = torch.empty_like(src)
+    idx = torch.randperm(m, device="cuda").int()
+    ga, sa = GatherAll(), ScatterAll()
+    msg = timed(lambda: ga.gather(tv.Tensor(dst), tv.Tensor(src), tv.Tensor(idx)), 10)
+    by = 2.0 * m * 128 + m * 4
+    out["gather_4M_rows_128B"] = {"ms": msg, "gbs": by / msg / 1e6, "frac_of_hbm": by / msg / 1e6 / peak_bw}
+    msc = timed(lambda: sa.scatter(tv.Tensor(dst), tv.Tensor(src), tv.Tensor(idx)), 10)
+    by = 3.0 * m * 128 + m * 4
+    out["scatter_add_4M_rows_128B"] = {"ms": msc, "gbs": by / msc / 1e6, "frac_of_hbm": by / msc / 1e6 / peak_bw}
+    del a, b, c, src, dst
+    torch.cuda.empty_cache()
     return out
 
 
@@ -533,7 +623,9 @@ def run_b200(args, rank, world, dist):
                         "peak_gbs": peak_bw, "frac": hbm_achieved / peak_bw}}
 
     # ---------------------------------------------------------------- batched / served forms (N = 1)
-    batched = served = None
+    batched = served = aux = None
+    if world == 1 and not args.no_aux:
+        aux = run_aux(*_peaks()[:2])
     if world == 1 and not args.no_batched:
         batched = run_batched()
     if world == 1 and not args.no_served:
@@ -577,6 +669,7 @@ def run_b200(args, rank, world, dist):
                 "steps": n_e2e, "pipelined_streams": 3, "buffer_sets": NBUF},
             "cpu_baseline": cpu,
             "batched": batched,
+            "aux": aux,
             "served": served,
             "gpu_launches": 5 * args.steps,
             "clocks": clocks,
@@ -594,6 +687,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end loop (profiling)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-cloud grouped vs sequential run")
     ap.add_argument("--no-served", action="store_true", help="skip the serving point (800 req/s)")
+    ap.add_argument("--no-aux", action="store_true", help="skip the GEMM / gather / scatter timings")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -563,7 +563,8 @@ static int plan_gemm(const sc_gemm_params *p, scb::GemmArgs *a) {
   if (p->shuffle_type == SC_SHUFFLE_AB && !(p->trans_a && !p->trans_b))
     return fail(SC_RUNTIME, "shuffle AB must be nt, i.e. backward weight");
   if (p->shuffle_type < 0 || p->shuffle_type > 2) return fail(SC_RUNTIME, "unknown shuffle type");
-  if (p->split_k_slices > 1) return fail(SC_RUNTIME, "algo don't support splitk but you provide split_k_slices > 1. %d", p->split_k_slices);
+  if (p->split_k_slices > 1 && p->shuffle_type == SC_SHUFFLE_AC)
+    return fail(SC_RUNTIME, "algo don't support splitk but you provide split_k_slices > 1. %d", p->split_k_slices);
   if (p->m < 0 || p->n < 0 || p->k < 0) return fail(SC_INVALID_ARG, "bad m, n, k");
   const int di = p->dtype_a;
   if (p->dtype_b != di) return fail(SC_RUNTIME, "Can't Found Algorithm: dtype_a != dtype_b");
@@ -600,6 +601,9 @@ static int plan_gemm(const sc_gemm_params *p, scb::GemmArgs *a) {
   a->epi.mode = 0;
   a->epi.src = p->d != nullptr ? p->d : p->c;
   a->epi.src_ld = p->d != nullptr ? p->ldd : p->ldc;
+  a->split_k = p->split_k_slices > 1 ? p->split_k_slices : 1;
+  if (a->split_k > 1 && !(scb::dense_gemm_supported(*a) || p->shuffle_type == SC_SHUFFLE_AB))
+    return fail(SC_RUNTIME, "algo don't support splitk but you provide split_k_slices > 1. %d", p->split_k_slices);
   return SC_OK;
 }
 

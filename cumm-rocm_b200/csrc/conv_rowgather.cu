@@ -131,20 +131,35 @@ __device__ __forceinline__ void load_src(const TOut *p, float *v) {
   }
 }
 
+// One 32-byte store (a whole DRAM sector: no partial-sector merge in L2).
+__device__ __forceinline__ void st_global_v8(void *p, const uint32_t *w) {
+  asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "r"(w[0]), "r"(w[1]), "r"(w[2]),
+               "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7])
+               : "memory");
+}
+
+// Stores n values to p: 32-byte stores when p is 32-byte aligned, else 16-byte.
 template <int n, typename TOut>
 __device__ __forceinline__ void store_row(TOut *p, const float *v) {
-  if constexpr (sizeof(TOut) == 4) {
+  constexpr int kPer32 = 32 / sizeof(TOut);  // values per 32 bytes
+  static_assert(n % kPer32 == 0, "row chunk must be whole 32-byte units");
+  const bool a32 = (reinterpret_cast<uintptr_t>(p) & 31u) == 0;
 #pragma unroll
-    for (int i = 0; i < n; i += 4)
-      *reinterpret_cast<float4 *>(p + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
-  } else {
+  for (int i = 0; i < n; i += kPer32) {
+    uint32_t w[8];
+    if constexpr (sizeof(TOut) == 4) {
 #pragma unroll
-    for (int i = 0; i < n; i += 8) {
-      uint4 q;
-      TOut *h = reinterpret_cast<TOut *>(&q);
+      for (int j = 0; j < 8; ++j) w[j] = __float_as_uint(v[i + j]);
+    } else {
+      TOut *h = reinterpret_cast<TOut *>(w);
 #pragma unroll
-      for (int j = 0; j < 8; ++j) h[j] = from_f32<TOut>(v[i + j]);
-      *reinterpret_cast<uint4 *>(p + i) = q;
+      for (int j = 0; j < 16; ++j) h[j] = from_f32<TOut>(v[i + j]);
+    }
+    if (a32) {
+      st_global_v8(p + i, w);
+    } else {
+      *reinterpret_cast<uint4 *>(p + i) = make_uint4(w[0], w[1], w[2], w[3]);
+      *reinterpret_cast<uint4 *>(p + i + kPer32 / 2) = make_uint4(w[4], w[5], w[6], w[7]);
     }
   }
 }

@@ -6,8 +6,10 @@
 //   ShuffleAB: C = act(alpha * A[a_inds]^T @ B[b_inds] + beta * D)
 // (shape rules: cumm/gemm/nvrtc_code.py:80-125).
 //
-// 16-bit operands run on the two tcgen05 kernels of this library:
-//   * row-major A (NoShuffle without trans_a, ShuffleAC) is the row-gather
+// 16-bit operands run on tcgen05 kernels:
+//   * NoShuffle is the dense GEMM of gemm_dense.cu (2-D TMA tiles, either
+//     operand read in place K- or MN-major, optional parallel split-K);
+//   * ShuffleAC is the row-gather
 //     kernel in GEMM mode (kv = 1, one 128-byte K chunk per stage, TMEM
 //     accumulator, permuted-store epilogue); B is consumed K-major, so a
 //     row-major [k, n] B is transposed once into the workspace;
@@ -130,8 +132,10 @@ __global__ void transpose2d_kernel(const T *src, int64_t ld_src, T *dst, int64_t
 
 int64_t align256(int64_t x) { return (x + 255) & ~static_cast<int64_t>(255); }
 
-// Which tcgen05 kernel can run this GEMM: 0 none (SIMT), 1 row-gather, 2 reduction-gather.
+// Which tcgen05 kernel can run this GEMM: 0 none (SIMT), 1 row-gather,
+// 2 reduction-gather, 3 dense.
 int tc_route(const GemmArgs &a) {
+  if (dense_gemm_supported(a)) return 3;
   if (a.in_dtype != 12 && a.in_dtype != 7) return 0;
   if (a.out_dtype != 0 && a.out_dtype != 7 && a.out_dtype != 12) return 0;
   const int64_t es = 2;
@@ -172,6 +176,7 @@ cudaError_t launch_simt_any(const GemmArgs &a, cudaStream_t s) {
 
 int64_t gemm_workspace_bytes(const GemmArgs &a) {
   const int route = tc_route(a);
+  if (route == 3) return dense_gemm_splits(a) > 1 ? align256(a.m * a.n * 4) : 0;
   if (route == 1) return a.trans_b ? 0 : align256(a.n * a.k * 2);
   if (route == 2) {
     int64_t b = align256(a.m * a.n * 4);
@@ -186,6 +191,23 @@ cudaError_t launch_gemm(const GemmArgs &a, int num_sms, cudaStream_t s) {
   const int route = tc_route(a);
   if (route == 0) return launch_simt_any(a, s);
   uint8_t *ws = reinterpret_cast<uint8_t *>(a.ws);
+  if (route == 3) {
+    // a shape the tensor maps cannot describe runs on the SIMT kernel
+    if (dense_gemm_splits(a) <= 1) {
+      cudaError_t e = launch_dense_gemm(a, nullptr, num_sms, s);
+      return e == cudaErrorInvalidValue ? launch_simt_any(a, s) : e;
+    }
+    // parallel split-K: partial tiles add into a zeroed fp32 [m, n], then the
+    // finalize pass applies act(alpha * sum + beta * D) and converts
+    float *acc = reinterpret_cast<float *>(ws);
+    cudaError_t e = cudaMemsetAsync(acc, 0, a.m * a.n * 4, s);
+    if (e != cudaSuccess) return e;
+    e = launch_dense_gemm(a, acc, num_sms, s);
+    if (e == cudaErrorInvalidValue) return launch_simt_any(a, s);
+    if (e != cudaSuccess) return e;
+    return launch_wgrad_finalize(acc, a.c, a.ldc, a.out_dtype, static_cast<int>(a.m), 1,
+                                 static_cast<int>(a.n), 1u, a.epi, s);
+  }
   if (route == 1) {
     const uint8_t *bt = a.b;
     int64_t ldbt = a.ldb;
@@ -277,6 +299,7 @@ cudaError_t launch_gemm(const GemmArgs &a, int num_sms, cudaStream_t s) {
   w.ws = acc;
   w.in_dtype = a.in_dtype;
   w.err = a.err;
+  w.split_k = a.split_k > 1 ? a.split_k : 0;
   e = launch_conv_wgrad(w, num_sms, s);
   if (e != cudaSuccess) return e;
   return launch_wgrad_finalize(acc, a.c, a.ldc, a.out_dtype, static_cast<int>(a.m), 1,

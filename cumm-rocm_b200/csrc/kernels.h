@@ -154,11 +154,17 @@ struct GemmArgs {
   int in_dtype;              // SC_BFLOAT16 / SC_FLOAT16 / SC_FLOAT32
   int out_dtype;
   EpiParams epi;
-  float *ws;                 // fp32 [m, n] accumulation workspace (ShuffleAB / trans_a)
+  float *ws;                 // fp32 [m, n] accumulation workspace (ShuffleAB, split-K)
   int *err;
+  int split_k;               // K splits (1 = none): dense route and ShuffleAB only
 };
 cudaError_t launch_gemm(const GemmArgs &a, int num_sms, cudaStream_t stream);
 int64_t gemm_workspace_bytes(const GemmArgs &a);
+// Dense tcgen05 GEMM (NoShuffle, 16-bit operands): whether it takes `a`, its
+// K-split count, and the launch (split_ws: zeroed fp32 [m, n] when splits > 1).
+bool dense_gemm_supported(const GemmArgs &a);
+int dense_gemm_splits(const GemmArgs &a);
+cudaError_t launch_dense_gemm(const GemmArgs &a, float *split_ws, int num_sms, cudaStream_t stream);
 
 // ------------------------------------------------------------------ gather / scatter
 // out[i] = in[indices[i]] (rows of row_bytes bytes), and

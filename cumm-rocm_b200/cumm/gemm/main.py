@@ -112,6 +112,11 @@ class GemmMainUnitTest:
         st = ShuffleStrideType(desp.shuffle_type)
         if tc and st != ShuffleStrideType.kNoShuffle:
             raise RuntimeError("trans_c is only supported without shuffle")
+        if tc:
+            # C stored transposed: C^T = op(B)^T op(A)^T, i.e. the same GEMM with
+            # the operands swapped and their transposes flipped
+            # (cumm/gemm/nvrtc_code.py:62-68)
+            a, b, ta, tb = b, a, not tb, not ta
         a_inds = params.a_inds if not params.a_inds.empty() else None
         b_inds = params.b_inds if not params.b_inds.empty() else None
         c_inds = params.c_inds if not params.c_inds.empty() else None
