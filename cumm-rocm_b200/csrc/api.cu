@@ -113,9 +113,16 @@ struct ConvPlan {
   int64_t ws_min = 0;    // what a call cannot run without
 };
 
-// Workspace head of the tcgen05 forward / backward-input kernels: the tile
-// counter of their dynamic scheduler (zeroed per call).
+// Workspace head of the tcgen05 forward / backward-input kernels (zeroed per
+// call): the tile counter of their dynamic scheduler, then the histogram and
+// block counter of the largest-first tile order.  The per-tile offset counts
+// and the order itself follow, ceil(N / 128) ints each.
 constexpr int64_t kSchedBytes = 256;
+
+int64_t sched_bytes(int64_t N) {
+  const int64_t m_tiles = (N + 127) / 128;
+  return kSchedBytes + 2 * align256(m_tiles * 4);
+}
 
 int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
   if (p == nullptr) return fail(SC_INVALID_ARG, "params is null");
@@ -203,7 +210,7 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
       return fail(SC_RUNTIME, "Can't Found Algorithm: C=%lld K=%lld not tiled by the tcgen05 kernel "
                   "(C*sizeof in {16,32,64} or a multiple of 16 >= 128 bytes; K %% 16 == 0)",
                   (long long)p->C, (long long)p->K);
-    plan->ws_bytes = kSchedBytes;  // optional: without it tiles are dealt statically
+    plan->ws_bytes = sched_bytes(p->N);  // optional: without it tiles are dealt statically
     return SC_OK;
   }
   if (op == SC_CONV_BACKWARD_INPUT) {
@@ -213,7 +220,7 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
     if (!rowgather_width_ok(p->K * esize(di)) || p->C % 16)
       return fail(SC_RUNTIME, "Can't Found Algorithm: K=%lld C=%lld not tiled by the tcgen05 kernel",
                   (long long)p->K, (long long)p->C);
-    plan->ws_bytes = kSchedBytes + align256(p->K * p->kv * p->C * esize(di));
+    plan->ws_bytes = sched_bytes(p->N) + align256(p->K * p->kv * p->C * esize(di));
     plan->ws_min = plan->ws_bytes;
     return SC_OK;
   }
@@ -373,9 +380,13 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     scb::ConvRowGatherArgs a{};
     uint8_t *ws = static_cast<uint8_t *>(p->workspace);
     if (ws != nullptr && p->workspace_bytes >= plan.ws_bytes) {
-      e = cudaMemsetAsync(ws, 0, sizeof(int), s);
+      e = cudaMemsetAsync(ws, 0, 35 * sizeof(int), s);
       if (e != cudaSuccess) return cuda_fail(e, "zero tile counter");
+      const int64_t order_bytes = align256((p->N + 127) / 128 * 4);
       a.tile_counter = reinterpret_cast<int *>(ws);
+      a.sched_head = reinterpret_cast<int *>(ws) + 1;
+      a.tile_pc = reinterpret_cast<int32_t *>(ws + kSchedBytes);
+      a.tile_order = reinterpret_cast<int32_t *>(ws + kSchedBytes + order_bytes);
     }
     a.a_base = static_cast<const uint8_t *>(fwd ? p->input : p->output);
     a.a_rows = fwd ? p->n_in : p->n_out;
@@ -400,10 +411,10 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     if (fwd || b_mn) {
       a.b_base = static_cast<const uint8_t *>(p->weight);
     } else {
-      e = scb::launch_transpose_weight(p->weight, ws + kSchedBytes, static_cast<int>(p->K), p->kv,
+      e = scb::launch_transpose_weight(p->weight, ws + sched_bytes(p->N), static_cast<int>(p->K), p->kv,
                                        static_cast<int>(p->C), es, s);
       if (e != cudaSuccess) return cuda_fail(e, "weight transpose launch");
-      a.b_base = ws + kSchedBytes;
+      a.b_base = ws + sched_bytes(p->N);
     }
     a.b_mn = b_mn ? 1 : 0;
     // B rows: [n, kv, red] (K-major), or for b_mn the weight's [red, kv, n]

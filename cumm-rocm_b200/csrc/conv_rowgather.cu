@@ -110,6 +110,97 @@ struct KParams {
 
 __device__ __forceinline__ void flag_error(int *err, int bits) { atomicOr(err, bits); }
 
+// ------------------------------------------------------------------ largest-first tile schedule
+// A 128-row tile costs one chunk per (offset it visits, column block), and on
+// the mask-sorted rows that count varies from a few offsets to all of them.
+// Handing tiles out in mask order leaves the pipelines that drew the heavy
+// tiles running alone at the end; handing them out heaviest first (the LPT
+// rule) evens the pipelines out.  This kernel writes that order: one warp per
+// tile ORs the tile's mask words (the kernels' tile mask: mask_filter, and
+// brev for backward-input) and counts its offsets into a histogram; the last
+// block to finish turns the histogram into descending bin starts and places
+// every tile (a counting sort; the order inside a bin is arbitrary and does
+// not affect any result, since each tile is computed by one pipeline alone).
+constexpr int kOrderWarps = 32;
+
+__global__ void __launch_bounds__(kOrderWarps * 32)
+    tile_order_kernel(const uint32_t *__restrict__ mask, int64_t M, uint32_t filter, int reverse, int kv,
+                      int64_t m_tiles, int *__restrict__ head, int32_t *__restrict__ tile_pc,
+                      int32_t *__restrict__ order) {
+  int *hist = head;        // [33]
+  int *done = head + 33;   // blocks finished
+  __shared__ int start[33];
+  __shared__ int last;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * kOrderWarps + warp;
+  if (t < m_tiles) {
+    uint32_t v = 0u;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t rq = t * kTileM + q * 32 + lane;
+      if (rq < M) v |= mask ? __ldg(mask + rq) : 1u;
+    }
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, sh);
+    uint32_t tm = v & filter;
+    if (reverse) tm = __brev(tm) >> (32 - kv);
+    if (lane == 0) {
+      const int pc = __popc(tm);
+      tile_pc[t] = pc;
+      atomicAdd(hist + pc, 1);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(done, 1) == static_cast<int>(gridDim.x) - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int b = 32; b >= 0; --b) {
+      start[b] = acc;
+      acc += __ldcg(hist + b);
+    }
+  }
+  __syncthreads();
+  // eight tiles per thread per pass, loads first
+  constexpr int kPer = 8;
+  for (int64_t base = 0; base < m_tiles; base += static_cast<int64_t>(blockDim.x) * kPer) {
+    int pc[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int64_t i = base + j * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+      pc[j] = i < m_tiles ? __ldcg(tile_pc + i) : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      if (pc[j] < 0) continue;
+      const int64_t i = base + j * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+      order[atomicAdd(&start[pc[j]], 1)] = static_cast<int32_t>(i);
+    }
+  }
+}
+
+cudaError_t launch_tile_order(const ConvRowGatherArgs &a, cudaStream_t stream) {
+  const int64_t m_tiles = (a.M + kTileM - 1) / kTileM;
+  if (m_tiles == 0) return cudaSuccess;
+  const int64_t blocks = (m_tiles + kOrderWarps - 1) / kOrderWarps;
+  tile_order_kernel<<<static_cast<unsigned>(blocks), kOrderWarps * 32, 0, stream>>>(
+      a.mask, a.M, a.mask_filter, a.reverse, a.kv, m_tiles, a.sched_head, a.tile_pc, a.tile_order);
+  return cudaGetLastError();
+}
+
+// Tile (row tile x column tile) at schedule position d: the d-th of the
+// largest-first order when it exists, else d itself.
+__device__ __forceinline__ int64_t scheduled_tile(const ConvRowGatherArgs &A, int64_t d) {
+  if (A.tile_order == nullptr) return d;
+  const int64_t mt = d / A.n_tiles;
+  return static_cast<int64_t>(__ldg(A.tile_order + mt)) * A.n_tiles + d % A.n_tiles;
+}
+
 
 // ------------------------------------------------------------------ epilogue helpers
 template <int n, typename TOut>
@@ -331,7 +422,7 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
           const int64_t d = A.tile_counter
                                 ? static_cast<int64_t>(next_draw >= 0 ? next_draw : atomicAdd(A.tile_counter, 1))
                                 : static_cast<int64_t>(blockIdx.x) + static_cast<int64_t>(it) * gridDim.x;
-          t = d < P.num_tiles ? static_cast<int>(d) : -1;
+          t = d < P.num_tiles ? static_cast<int>(scheduled_tile(A, d)) : -1;
           // While more tiles remain than there are CTAs, the following tile is
           // drawn now, so the atomic's round trip overlaps this tile's loads;
           // near the end (or on a grid with few tiles) a CTA holding two
@@ -921,6 +1012,20 @@ __device__ __forceinline__ TileMasks reduce_masks(const ConvRowGatherArgs &A, co
   return t;
 }
 
+// The it-th tile of the strand at schedule position pos, or -1 past the end.
+// With the largest-first order the positions take the tiles in a snake
+// (0 .. nstr-1, then nstr-1 .. 0, ...), so the strand that drew the heaviest
+// tile of one round draws the lightest of the next; without it, every nstr-th
+// tile.
+__device__ __forceinline__ int64_t strand_tile(const KParams &P, int64_t pos, int64_t nstr, int64_t it) {
+  if (P.a.tile_order == nullptr) {
+    const int64_t d = it * nstr + pos;
+    return d < P.num_tiles ? d : -1;
+  }
+  const int64_t d = it * nstr + ((it & 1) ? nstr - 1 - pos : pos);
+  return d < P.num_tiles ? scheduled_tile(P.a, d) : -1;
+}
+
 template <bool kF8, typename TOut>
 __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KParams P) {
   extern __shared__ uint8_t smem_raw[];
@@ -975,10 +1080,15 @@ __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KPara
     uint64_t *acc_empty = acc_full + 2;
     uint64_t *tile_bar = acc_full + 4;
     uint64_t *drain_bar = acc_full + 6;
-    const int64_t first = static_cast<int64_t>(blockIdx.x) * kStrands + s;
+    // this strand's position in the schedule: consecutive positions sit on
+    // consecutive CTAs (so on different SMs)
+    const int64_t pos = static_cast<int64_t>(s) * gridDim.x + blockIdx.x;
     const uint32_t ring = smem_base + static_cast<uint32_t>(s * S) * P.stage_bytes;
     uint32_t w[4] = {0u, 0u, 0u, 0u};
-    if (first < P.num_tiles) load_mask_words(A, first / A.n_tiles, lane, w);
+    {
+      const int64_t t0 = strand_tile(P, pos, nstr, 0);
+      if (t0 >= 0) load_mask_words(A, t0 / A.n_tiles, lane, w);
+    }
     if (role < kSProd) {
       // ---------------------------------------------------------------- producers
       // Warp pw gathers rows [32 pw, 32 pw + 32) of every chunk: lanes 0-7
@@ -994,8 +1104,9 @@ __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KPara
       const uint32_t a_tx = 32u * 128u;
       const uint32_t b_tx = static_cast<uint32_t>(A.BN) * 128u;
       const int r0 = pw * 32 + lane * 4;
-      // cursor (warp-uniform): tile, offsets not started yet, current offset / column block
-      int64_t c_tile = first - nstr, c_tile_m = 0;
+      // cursor (warp-uniform): tile (the strand's c_it-th), offsets not
+      // started yet, current offset / column block
+      int64_t c_it = -1, c_tile = -1, c_tile_m = 0;
       uint32_t c_mm = 0u, c_sub = 0u;
       int c_k = 0, c_cb = 0, c_n0 = 0;
       bool c_valid = true;
@@ -1003,13 +1114,14 @@ __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KPara
       // mask_output for each tile entered)
       auto next_tile = [&]() {
         for (;;) {
-          c_tile += nstr;
-          if (c_tile >= P.num_tiles) {
+          c_tile = strand_tile(P, pos, nstr, ++c_it);
+          if (c_tile < 0) {
             c_valid = false;
             return;
           }
           const TileMasks t = reduce_masks(A, w);
-          if (c_tile + nstr < P.num_tiles) load_mask_words(A, (c_tile + nstr) / A.n_tiles, lane, w);
+          const int64_t t_next = strand_tile(P, pos, nstr, c_it + 1);
+          if (t_next >= 0) load_mask_words(A, t_next / A.n_tiles, lane, w);
           c_tile_m = c_tile / A.n_tiles;
           const int n_tile = static_cast<int>(c_tile % A.n_tiles);
           c_n0 = n_tile * A.BN;
@@ -1127,13 +1239,14 @@ __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KPara
       const uint64_t b_kstep = P.b_mn ? 128 : 2;
       uint32_t stage = 0, fph = 0;
       bool issued = false, ok = true;
-      int64_t tile = first;
-      for (int it = 0;; ++it, tile += nstr) {
-        const bool have = tile < P.num_tiles;
+      for (int it = 0;; ++it) {
+        const int64_t tile = strand_tile(P, pos, nstr, it);
+        const bool have = tile >= 0;
         int nch = 0;
         if (have) {
           const TileMasks tmk = reduce_masks(A, w);
-          if (tile + nstr < P.num_tiles) load_mask_words(A, (tile + nstr) / A.n_tiles, lane, w);
+          const int64_t t_next = strand_tile(P, pos, nstr, it + 1);
+          if (t_next >= 0) load_mask_words(A, t_next / A.n_tiles, lane, w);
           nch = __popc(tmk.tm) * P.cpo;
         }
         if (lane == 0) {
@@ -1373,6 +1486,10 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
     const size_t smem = 1024 + P.bar_off + 512;
     const int64_t ctas = (P.num_tiles + kStrands - 1) / kStrands;
     const int grid = static_cast<int>(ctas < 2 * num_sms ? ctas : 2 * num_sms);
+    if (a.tile_order != nullptr) {
+      const cudaError_t e = launch_tile_order(a, stream);
+      if (e != cudaSuccess) return e;
+    }
     if (a.in_dtype == 14) {
       P.idesc = make_idesc(128, a.BN, 0u, false, false);
       switch (a.out_dtype) {
@@ -1413,6 +1530,12 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
   P.bar_off = P.idx_off + P.idx_buf_bytes * idx_stages;
   const size_t smem = 1024 + P.bar_off + bar_bytes;
   if (P.num_tiles == 0) return cudaSuccess;
+  if (a.tile_order != nullptr && a.tile_counter != nullptr) {
+    const cudaError_t e = launch_tile_order(a, stream);
+    if (e != cudaSuccess) return e;
+  } else {
+    P.a.tile_order = nullptr;
+  }
   const int64_t ctas = static_cast<int64_t>(pair ? 2 : 1) * num_sms;
   const int grid = static_cast<int>(P.num_tiles < ctas ? P.num_tiles : ctas);
   if (a.in_dtype == 14) {

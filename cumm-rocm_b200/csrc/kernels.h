@@ -64,6 +64,12 @@ struct ConvRowGatherArgs {
   int64_t out_rows;          // bound for output rows
   const int32_t *idx_sorted; // optional [kv, M]: indices[k][argsort[r]]
   int *tile_counter;         // optional, zero at launch: tiles handed out dynamically
+  // optional largest-first tile schedule (all three or none): sched_head
+  // points at 34 ints zeroed before the launch (33 histogram bins + a block
+  // counter), tile_pc and tile_order at ceil(M / 128) ints each
+  int *sched_head;
+  int32_t *tile_pc;
+  int32_t *tile_order;
   // backward-input with B = the [K, kv, C] weight itself: the slab of offset
   // k is rows j (reduction) x columns k * C + c (n), read MN-major by the
   // tensor core (no transposed copy); needs 16-bit data, red % 64 == 0 and

@@ -510,3 +510,55 @@ def test_strand_kernel_fp8_and_bad_index():
     db = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 128)
     with pytest.raises(RuntimeError, match="device error"):
         conv(ConvOpType.kForward, db, xb, wb, ob, bad, ms, order, sorted_indices=True)
+
+
+@pytest.mark.parametrize("use_sorted", [True, False])
+def test_tile_schedule_does_not_change_results(use_sorted):
+    """With a workspace the forward hands its 128-row tiles out heaviest
+    first (a per-call counting sort of the tiles by the offsets they visit);
+    without one (a workspace is optional for the forward) it deals them in
+    mask order.  Each tile is computed by one pipeline alone, so both give
+    bit-identical outputs and mask_output, on the strand kernel (sorted index
+    table) and on the row-gather kernel, and match the FP64 oracle."""
+    import ctypes
+    from cumm import _lib
+    from cumm.conv.main import ConvMainUnitTest, build_conv_params_c
+    from cumm.spconv_ops import build_pair_table
+    from cumm.tensorview.gemm import ConvParams
+    n, C, K = 40000, 64, 64
+    coords = vg.lidar_voxels(n, seed=11)
+    pt = build_pair_table(torch.from_numpy(coords).cuda(), vg.KITTI_SHAPE)
+    rng = np.random.default_rng(11)
+    x = dev(rng.standard_normal((n, C)).astype(np.float32), torch.bfloat16)
+    w = dev(vg.kaiming_uniform(K, 27, C, 11), torch.bfloat16)
+    outs, mos = [], []
+    for with_ws in (True, False):
+        p = ConvParams(3, ConvOpType.kForward)
+        p.conv_algo_desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 32)
+        o = torch.full((n, K), float("nan"), dtype=torch.bfloat16, device="cuda")
+        mo = tv.zeros([(n + 31) // 32], tv.uint32, 0)
+        p.input, p.weight, p.output = tv.Tensor(x), tv.Tensor(w), tv.Tensor(o)
+        p.indices = tv.Tensor(pt.pairs_fwd)
+        p.mask = tv.Tensor(pt.masks_fwd[0], tv.uint32)
+        p.mask_argsort = tv.Tensor(pt.argsorts_fwd[0])
+        p.mask_output = mo
+        if use_sorted:
+            p.indices_sorted = tv.Tensor(pt.sorted_indices("fwd"))
+        if with_ws:
+            ConvMainUnitTest(sync_check=True).implicit_gemm2(p)
+        else:
+            cp, _info = build_conv_params_c(p)
+            cp.flags |= _lib.SC_FLAG_SYNC_CHECK
+            cp.workspace, cp.workspace_bytes = None, 0
+            _lib.check(_lib.load().sc_conv_implicit_gemm(ctypes.byref(cp)))
+        torch.cuda.synchronize()
+        outs.append(o.float().cpu())
+        mos.append(mo.numpy().copy())
+    assert not torch.isnan(outs[0]).any()
+    assert torch.equal(outs[0], outs[1])
+    assert np.array_equal(mos[0], mos[1])
+    m = pt.masks_fwd[0].cpu().numpy().view(np.uint32)
+    order = pt.argsorts_fwd[0].cpu().numpy()
+    ref, mo_ref = co.conv_fwd_masked(to64(x), to64(w), pt.pairs_fwd.cpu().numpy(), m, order, 32)
+    _assert_close(outs[0].double().numpy(), ref, TOL_16)
+    assert np.array_equal(mos[0], mo_ref)

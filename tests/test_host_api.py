@@ -58,9 +58,13 @@ def _ws(cp):
 
 
 def test_conv_validation_codes():
-    assert _ws(_fake_conv())[:2] == (0, 256)          # fwd: tile counter (optional)
+    # fwd: tile counter and largest-first schedule (optional): a 256-byte head,
+    # then ceil(N / 128) per-tile offset counts and the tile order, each
+    # rounded up to 256 bytes (N = 1000: 8 tiles)
+    sched = 256 + 2 * 256
+    assert _ws(_fake_conv())[:2] == (0, sched)
     rc, n, _ = _ws(_fake_conv(1))
-    assert rc == 0 and n == 256 + 64 * 27 * 64 * 2    # dgrad: tile counter + transposed weight
+    assert rc == 0 and n == sched + 64 * 27 * 64 * 2  # dgrad: schedule + transposed weight
     rc, n, _ = _ws(_fake_conv(2))
     assert rc == 0 and n == 64 * 27 * 64 * 4          # wgrad: fp32 accumulation
     rc, _, msg = _ws(_fake_conv(0, N=999))
