@@ -447,6 +447,8 @@ def run_b200(args, rank, world, dist):
         p.mask_argsort = tv.Tensor(pt_.argsorts_fwd[0])
         p.indices_sorted = tv.Tensor(pt_.sorted_indices(
             "bwd" if op == ConvOpType.kBackwardInput else "fwd"))
+        if op != ConvOpType.kBackwardWeight:
+            p.tile_order = tv.Tensor(pt_.tile_order("fwd"))
         p.stream = sptr
         cp, _ = build_conv_params_c(p)
         need = ctypes.c_int64(0)
@@ -572,6 +574,8 @@ def run_b200(args, rank, world, dist):
                 p.mask_argsort = tv.Tensor(ptd.argsorts_fwd[0])
                 p.indices_sorted = tv.Tensor(ptd.sorted_indices(
                     "bwd" if op == ConvOpType.kBackwardInput else "fwd"))
+                if op != ConvOpType.kBackwardWeight:
+                    p.tile_order = tv.Tensor(ptd.tile_order("fwd"))
                 p.stream = cptr
                 cmt.implicit_gemm2(p)
                 if op == ConvOpType.kForward:

@@ -379,14 +379,18 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     const int64_t ncols = fwd ? p->K : p->C;  // output columns
     scb::ConvRowGatherArgs a{};
     uint8_t *ws = static_cast<uint8_t *>(p->workspace);
+    // schedule state in the workspace head (zeroed by the launcher); the
+    // largest-first order is the caller's when given, else computed here
     if (ws != nullptr && p->workspace_bytes >= plan.ws_bytes) {
-      e = cudaMemsetAsync(ws, 0, 35 * sizeof(int), s);
-      if (e != cudaSuccess) return cuda_fail(e, "zero tile counter");
       const int64_t order_bytes = align256((p->N + 127) / 128 * 4);
       a.tile_counter = reinterpret_cast<int *>(ws);
       a.sched_head = reinterpret_cast<int *>(ws) + 1;
       a.tile_pc = reinterpret_cast<int32_t *>(ws + kSchedBytes);
       a.tile_order = reinterpret_cast<int32_t *>(ws + kSchedBytes + order_bytes);
+    }
+    if (p->tile_order != nullptr) {
+      a.tile_order = p->tile_order;
+      a.order_given = 1;
     }
     a.a_base = static_cast<const uint8_t *>(fwd ? p->input : p->output);
     a.a_rows = fwd ? p->n_in : p->n_out;
@@ -812,6 +816,38 @@ int sc_sort_indices(const int32_t *indices, int32_t kv, int64_t N, const int32_t
   cudaError_t e = scb::sort_indices(indices, kv, N, argsort, indices_sorted,
                                     static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "sort_indices");
+  return SC_OK;
+}
+
+int sc_tile_order_workspace_size(int64_t N, int64_t *bytes) {
+  g_last_error.clear();
+  if (bytes == nullptr) return fail(SC_INVALID_ARG, "bytes is null");
+  if (N < 0) return fail(SC_INVALID_ARG, "N must be >= 0");
+  *bytes = kSchedBytes + align256((N + 127) / 128 * 4);
+  return SC_OK;
+}
+
+int sc_tile_order(const uint32_t *mask, int64_t N, uint32_t mask_filter, int32_t kv, int32_t reverse,
+                  int32_t *tile_order, void *workspace, int64_t workspace_bytes, void *stream) {
+  g_last_error.clear();
+  if (N < 0) return fail(SC_INVALID_ARG, "N must be >= 0");
+  if (N == 0) return SC_OK;
+  if (mask == nullptr || tile_order == nullptr) return fail(SC_INVALID_ARG, "mask and tile_order must not be null");
+  if (kv < 1 || kv > 32) return fail(SC_INVALID_ARG, "kernel volume %d not supported (1..32)", kv);
+  const int64_t need = kSchedBytes + align256((N + 127) / 128 * 4);
+  if (workspace == nullptr || workspace_bytes < need)
+    return fail(SC_RUNTIME, "workspace at least %lld bytes.", (long long)need);
+  int *err = nullptr;
+  int sms = 0;
+  int rc = device_state(&err, &sms);
+  if (rc != SC_OK) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  uint8_t *ws = static_cast<uint8_t *>(workspace);
+  cudaError_t e = cudaMemsetAsync(ws, 0, 34 * sizeof(int), s);
+  if (e != cudaSuccess) return cuda_fail(e, "zero tile order histogram");
+  e = scb::launch_tile_order(mask, N, mask_filter, reverse ? 1 : 0, kv, reinterpret_cast<int *>(ws),
+                             reinterpret_cast<int32_t *>(ws + kSchedBytes), tile_order, s);
+  if (e != cudaSuccess) return cuda_fail(e, "tile order launch");
   return SC_OK;
 }
 

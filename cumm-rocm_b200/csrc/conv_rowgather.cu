@@ -117,10 +117,11 @@ __device__ __forceinline__ void flag_error(int *err, int bits) { atomicOr(err, b
 // tiles running alone at the end; handing them out heaviest first (the LPT
 // rule) evens the pipelines out.  This kernel writes that order: one warp per
 // tile ORs the tile's mask words (the kernels' tile mask: mask_filter, and
-// brev for backward-input) and counts its offsets into a histogram; the last
-// block to finish turns the histogram into descending bin starts and places
-// every tile (a counting sort; the order inside a bin is arbitrary and does
-// not affect any result, since each tile is computed by one pipeline alone).
+// brev for backward-input) and counts its offsets into the block's histogram,
+// which the block adds to the global one; the last block to finish turns the
+// histogram into descending bin starts and places every tile (a counting
+// sort; the order inside a bin is arbitrary and does not affect any result,
+// since each tile is computed by one pipeline alone).
 constexpr int kOrderWarps = 32;
 
 __global__ void __launch_bounds__(kOrderWarps * 32)
@@ -129,9 +130,11 @@ __global__ void __launch_bounds__(kOrderWarps * 32)
                       int32_t *__restrict__ order) {
   int *hist = head;        // [33]
   int *done = head + 33;   // blocks finished
-  __shared__ int start[33];
+  __shared__ int bins[33];
   __shared__ int last;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x < 33) bins[threadIdx.x] = 0;
+  __syncthreads();
   const int64_t t = static_cast<int64_t>(blockIdx.x) * kOrderWarps + warp;
   if (t < m_tiles) {
     uint32_t v = 0u;
@@ -147,9 +150,11 @@ __global__ void __launch_bounds__(kOrderWarps * 32)
     if (lane == 0) {
       const int pc = __popc(tm);
       tile_pc[t] = pc;
-      atomicAdd(hist + pc, 1);
+      atomicAdd(&bins[pc], 1);
     }
   }
+  __syncthreads();
+  if (threadIdx.x < 33 && bins[threadIdx.x] != 0) atomicAdd(hist + threadIdx.x, bins[threadIdx.x]);
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -158,11 +163,14 @@ __global__ void __launch_bounds__(kOrderWarps * 32)
   __syncthreads();
   if (!last) return;
   __threadfence();
+  if (threadIdx.x < 33) bins[threadIdx.x] = __ldcg(hist + threadIdx.x);
+  __syncthreads();
   if (threadIdx.x == 0) {
     int acc = 0;
     for (int b = 32; b >= 0; --b) {
-      start[b] = acc;
-      acc += __ldcg(hist + b);
+      const int c = bins[b];
+      bins[b] = acc;
+      acc += c;
     }
   }
   __syncthreads();
@@ -179,26 +187,25 @@ __global__ void __launch_bounds__(kOrderWarps * 32)
     for (int j = 0; j < kPer; ++j) {
       if (pc[j] < 0) continue;
       const int64_t i = base + j * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-      order[atomicAdd(&start[pc[j]], 1)] = static_cast<int32_t>(i);
+      order[atomicAdd(&bins[pc[j]], 1)] = static_cast<int32_t>(i);
     }
   }
 }
 
-cudaError_t launch_tile_order(const ConvRowGatherArgs &a, cudaStream_t stream) {
-  const int64_t m_tiles = (a.M + kTileM - 1) / kTileM;
-  if (m_tiles == 0) return cudaSuccess;
-  const int64_t blocks = (m_tiles + kOrderWarps - 1) / kOrderWarps;
-  tile_order_kernel<<<static_cast<unsigned>(blocks), kOrderWarps * 32, 0, stream>>>(
-      a.mask, a.M, a.mask_filter, a.reverse, a.kv, m_tiles, a.sched_head, a.tile_pc, a.tile_order);
-  return cudaGetLastError();
-}
-
 // Tile (row tile x column tile) at schedule position d: the d-th of the
-// largest-first order when it exists, else d itself.
+// largest-first order when it exists, else d itself.  An order entry outside
+// the row tiles (a caller-supplied order) sets the bad-index bit and maps to
+// the first row tile past the end, whose rows all lie beyond M, so every
+// role skips it.
 __device__ __forceinline__ int64_t scheduled_tile(const ConvRowGatherArgs &A, int64_t d) {
   if (A.tile_order == nullptr) return d;
-  const int64_t mt = d / A.n_tiles;
-  return static_cast<int64_t>(__ldg(A.tile_order + mt)) * A.n_tiles + d % A.n_tiles;
+  const int64_t q = d / A.n_tiles;
+  uint32_t mt = static_cast<uint32_t>(__ldg(A.tile_order + q));
+  if (mt >= static_cast<uint32_t>(A.m_tiles)) {
+    atomicOr(A.err, kErrBadIndex);
+    mt = static_cast<uint32_t>(A.m_tiles);
+  }
+  return static_cast<int64_t>(mt) * A.n_tiles + (d - q * A.n_tiles);
 }
 
 
@@ -1411,10 +1418,41 @@ cudaError_t launch_typed(const KParams &P, bool tma, bool gather, bool pair, int
 
 }  // namespace
 
+cudaError_t launch_tile_order(const uint32_t *mask, int64_t M, uint32_t filter, int reverse, int kv,
+                              int *head, int32_t *tile_pc, int32_t *order, cudaStream_t stream) {
+  const int64_t m_tiles = (M + kTileM - 1) / kTileM;
+  if (m_tiles == 0) return cudaSuccess;
+  const int64_t blocks = (m_tiles + kOrderWarps - 1) / kOrderWarps;
+  tile_order_kernel<<<static_cast<unsigned>(blocks), kOrderWarps * 32, 0, stream>>>(
+      mask, M, filter, reverse, kv, m_tiles, head, tile_pc, order);
+  return cudaGetLastError();
+}
+
+namespace {
+// Zeroes the schedule head (tile counter and histogram) and, unless the
+// caller gave an order, writes the largest-first order.
+cudaError_t prepare_schedule(const ConvRowGatherArgs &a, bool counter, cudaStream_t stream) {
+  if (a.order_given) {
+    if (!counter || a.tile_counter == nullptr) return cudaSuccess;
+    return cudaMemsetAsync(a.tile_counter, 0, sizeof(int), stream);
+  }
+  if (a.tile_order == nullptr) {
+    if (!counter || a.tile_counter == nullptr) return cudaSuccess;
+    return cudaMemsetAsync(a.tile_counter, 0, sizeof(int), stream);
+  }
+  // the head is the tile counter followed by the 34 ints of sched_head
+  cudaError_t e = cudaMemsetAsync(a.tile_counter, 0, 35 * sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  return launch_tile_order(a.mask, a.M, a.mask_filter, a.reverse, a.kv, a.sched_head, a.tile_pc,
+                           const_cast<int32_t *>(a.tile_order), stream);
+}
+}  // namespace
+
 cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaStream_t stream) {
   KParams P;
   P.a = a;
   const int64_t m_tiles = (a.M + kTileM - 1) / kTileM;
+  P.a.m_tiles = static_cast<int>(m_tiles);
   P.num_tiles = m_tiles * a.n_tiles;
   const int esz = a.in_dtype == 14 ? 1 : 2;
   const uint64_t red = static_cast<uint64_t>(a.a_row_bytes) / esz;
@@ -1486,8 +1524,8 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
     const size_t smem = 1024 + P.bar_off + 512;
     const int64_t ctas = (P.num_tiles + kStrands - 1) / kStrands;
     const int grid = static_cast<int>(ctas < 2 * num_sms ? ctas : 2 * num_sms);
-    if (a.tile_order != nullptr) {
-      const cudaError_t e = launch_tile_order(a, stream);
+    {
+      const cudaError_t e = prepare_schedule(a, false, stream);
       if (e != cudaSuccess) return e;
     }
     if (a.in_dtype == 14) {
@@ -1530,11 +1568,9 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
   P.bar_off = P.idx_off + P.idx_buf_bytes * idx_stages;
   const size_t smem = 1024 + P.bar_off + bar_bytes;
   if (P.num_tiles == 0) return cudaSuccess;
-  if (a.tile_order != nullptr && a.tile_counter != nullptr) {
-    const cudaError_t e = launch_tile_order(a, stream);
+  {
+    const cudaError_t e = prepare_schedule(a, true, stream);
     if (e != cudaSuccess) return e;
-  } else {
-    P.a.tile_order = nullptr;
   }
   const int64_t ctas = static_cast<int64_t>(pair ? 2 : 1) * num_sms;
   const int grid = static_cast<int>(P.num_tiles < ctas ? P.num_tiles : ctas);

@@ -64,12 +64,16 @@ struct ConvRowGatherArgs {
   int64_t out_rows;          // bound for output rows
   const int32_t *idx_sorted; // optional [kv, M]: indices[k][argsort[r]]
   int *tile_counter;         // optional, zero at launch: tiles handed out dynamically
-  // optional largest-first tile schedule (all three or none): sched_head
-  // points at 34 ints zeroed before the launch (33 histogram bins + a block
-  // counter), tile_pc and tile_order at ceil(M / 128) ints each
+  // optional largest-first tile schedule: tile_order holds ceil(M / 128)
+  // ints.  With order_given it was computed by the caller; otherwise the
+  // launcher computes it first, using sched_head (34 ints: 33 histogram bins
+  // and a block counter, zeroed by the launcher) and tile_pc (ceil(M / 128)
+  // ints).  tile_counter, when set, is zeroed by the launcher as well.
   int *sched_head;
   int32_t *tile_pc;
-  int32_t *tile_order;
+  const int32_t *tile_order;
+  int order_given;
+  int m_tiles;               // ceil(M / 128), set by the launcher
   // backward-input with B = the [K, kv, C] weight itself: the slab of offset
   // k is rows j (reduction) x columns k * C + c (n), read MN-major by the
   // tensor core (no transposed copy); needs 16-bit data, red % 64 == 0 and
@@ -77,6 +81,9 @@ struct ConvRowGatherArgs {
   int b_mn;
 };
 cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaStream_t stream);
+// head: 34 zeroed ints; tile_pc: m_tiles ints of scratch; order: m_tiles ints
+cudaError_t launch_tile_order(const uint32_t *mask, int64_t M, uint32_t filter, int reverse, int kv,
+                              int *head, int32_t *tile_pc, int32_t *order, cudaStream_t stream);
 
 // dgrad weight transposition W[K, kv, C] -> Wt[C, kv, K] (16-bit or 8-bit elements)
 cudaError_t launch_transpose_weight(const void *w, void *wt, int K, int kv, int C, int esize,

@@ -22,6 +22,7 @@ EXPORTS = (
     "sc_build_conv_pairs", "sc_sort_masks_split", "sc_sort_workspace_size",
     "sc_check_device_error", "sc_last_error", "sc_version", "sc_sort_indices",
     "sc_conv_wgrad_static_scratch", "sc_gather_rows", "sc_scatter_add_rows",
+    "sc_tile_order", "sc_tile_order_workspace_size",
 )
 
 c_i32, c_i64, c_u32, c_f32, c_vp = (ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32,
@@ -40,7 +41,7 @@ class ConvParamsC(ctypes.Structure):
         ("act_alpha", c_f32), ("act_beta", c_f32), ("act_type", c_i32), ("bias", c_vp),
         ("output_add", c_vp), ("scale", c_vp), ("split_k_slices", c_i32), ("flags", c_i32),
         ("workspace", c_vp), ("workspace_bytes", c_i64), ("stream", c_vp),
-        ("indices_sorted", c_vp), ("tile_n", c_i32),
+        ("indices_sorted", c_vp), ("tile_n", c_i32), ("tile_order", c_vp),
     ]
 
 
@@ -93,6 +94,8 @@ def load() -> ctypes.CDLL:
         lib.sc_sort_workspace_size.argtypes = [c_i64, P(c_i64)]
         lib.sc_check_device_error.argtypes = [c_vp, P(c_i32)]
         lib.sc_sort_indices.argtypes = [c_vp, c_i32, c_i64, c_vp, c_vp, c_vp]
+        lib.sc_tile_order_workspace_size.argtypes = [c_i64, P(c_i64)]
+        lib.sc_tile_order.argtypes = [c_vp, c_i64, c_u32, c_i32, c_i32, c_vp, c_vp, c_i64, c_vp]
         lib.sc_gather_rows.argtypes = [c_vp, c_vp, c_i64, c_vp, c_i64, c_i64, c_i32, c_i32, c_vp]
         lib.sc_scatter_add_rows.argtypes = [c_vp, c_i64, c_vp, c_vp, c_i64, c_i64, c_i32, c_i32,
                                             c_i32, c_vp]

@@ -146,6 +146,13 @@ def build_conv_params_c(params: ConvParams) -> Tuple[_lib.ConvParamsC, dict]:
         _check_dense(isorted, "indices_sorted")
         cp.indices_sorted = isorted.byte_pointer()
     cp.tile_n = int(getattr(params, "tile_n", 0) or 0)
+    torder = getattr(params, "tile_order", None)
+    if torder is not None and not torder.empty():
+        n_rows = int(params.indices.shape[1])
+        if torder.dtype != tv.int32 or list(torder.shape) != [(n_rows + 127) // 128]:
+            raise ValueError("tile_order must be int32 [ceil(N / 128)]")
+        _check_dense(torder, "tile_order")
+        cp.tile_order = torder.byte_pointer()
     return cp, {"kv": kv, "C": C, "K": K}
 
 

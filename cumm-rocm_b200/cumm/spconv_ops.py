@@ -172,6 +172,28 @@ class SpconvOps:
         return out
 
 
+    @staticmethod
+    def tile_order(mask, kv: int, mask_filter: int = 0xffffffff, reverse: bool = False,
+                   stream: int = 0):
+        """Largest-first order of the 128-row tiles of the sorted masks (the
+        optional ConvParams.tile_order): tiles by the number of offsets their
+        OR-ed masks visit, heaviest first."""
+        _lib.require_cuda()
+        lib = _lib.load()
+        m = _t(mask)
+        n = int(m.numel())
+        out = torch.empty(((n + 127) // 128,), dtype=torch.int32, device=m.device)
+        need = ctypes.c_int64(0)
+        _lib.check(lib.sc_tile_order_workspace_size(n, ctypes.byref(need)))
+        ws = torch.empty((max(int(need.value), 1),), dtype=torch.uint8, device=m.device)
+        _lib.check(lib.sc_tile_order(_vp(m), n, ctypes.c_uint32(mask_filter & 0xffffffff), kv,
+                                     1 if reverse else 0, _vp(out), _vp(ws), ws.numel(),
+                                     _stream(stream)))
+        if isinstance(mask, tv.Tensor):
+            return tv.Tensor(out, tv.int32)
+        return out
+
+
 def _as_i32(v: int) -> int:
     v &= 0xffffffff
     return v - (1 << 32) if v >= (1 << 31) else v
@@ -213,6 +235,20 @@ class PairTable:
             else:
                 order = self.argsorts_fwd[split] if self.subm else self.argsorts_bwd[split]
                 cache[key] = SpconvOps.sort_indices(self.pairs_bwd, order)
+        return cache[key]
+
+    def tile_order(self, which: str = "fwd", split: int = 0) -> torch.Tensor:
+        """Largest-first tile order (ConvParams.tile_order) for the masks
+        `which` uses: forward and (submanifold) backward-input share
+        masks_fwd[split], whose offset counts are the same in both directions;
+        a strided backward-input uses masks_bwd[split].  Cached per (which,
+        split)."""
+        cache = self.__dict__.setdefault("_order_cache", {})
+        key = ("fwd" if which == "fwd" or self.subm else "bwd", split)
+        if key not in cache:
+            masks = self.masks_fwd if key[0] == "fwd" else self.masks_bwd
+            cache[key] = SpconvOps.tile_order(masks[split], self.kv, self.split_masks[split]
+                                              if self.split_masks else 0xffffffff)
         return cache[key]
 
 

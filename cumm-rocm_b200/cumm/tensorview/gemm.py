@@ -413,3 +413,7 @@ class ConvParams:
         # extension: output-column tile of the tcgen05 fwd / dgrad kernels
         # (0 = widest); set by cumm.autotune, results are identical
         self.tile_n = 0
+        # extension: the order in which the tcgen05 fwd / dgrad kernels take
+        # their 128-row tiles (SpconvOps.tile_order, heaviest first); without
+        # it each call computes that order; results are identical
+        self.tile_order = Tensor()

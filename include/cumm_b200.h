@@ -131,6 +131,14 @@ typedef struct sc_conv_params {
    * columns up to 256); otherwise a multiple of 16, <= 256, dividing the
    * output width (K forward, C backward-input), else SC_INVALID_ARG. */
   int32_t tile_n;
+  /* Optional (may be NULL): the order in which the tcgen05 forward /
+   * backward-input kernels take their 128-row tiles, ceil(N / 128) int32
+   * entries, a permutation of 0 .. ceil(N / 128) - 1 as sc_tile_order writes
+   * it.  Results do not depend on it.  Without it (and with a workspace) each
+   * call computes the order itself, which costs a small kernel per call; an
+   * entry outside the range sets error bit 1 and its tile is skipped (the
+   * permutation property itself is not checked). */
+  const int32_t *tile_order;
 } sc_conv_params;
 
 /*
@@ -264,6 +272,18 @@ int sc_sort_workspace_size(int64_t n, int64_t *bytes);
  * that is reused by several convolutions). */
 int sc_sort_indices(const int32_t *indices, int32_t kv, int64_t N, const int32_t *argsort,
                     int32_t *indices_sorted, void *stream);
+
+/* Largest-first tile order for sc_conv_params.tile_order: the 128-row tiles
+ * of the mask-sorted rows ordered by the number of offsets they visit
+ * (popcount of the OR of their mask words AND mask_filter), heaviest first;
+ * ties in any order.  reverse = 1 gives the backward-input count (brev of the
+ * mask, kv bits), which equals the forward one for masks of kv bits, so one
+ * order serves both directions of a submanifold layer.  The workspace (size
+ * from sc_tile_order_workspace_size) is scratch of this call.  Asynchronous
+ * on `stream`. */
+int sc_tile_order_workspace_size(int64_t N, int64_t *bytes);
+int sc_tile_order(const uint32_t *mask, int64_t N, uint32_t mask_filter, int32_t kv, int32_t reverse,
+                  int32_t *tile_order, void *workspace, int64_t workspace_bytes, void *stream);
 
 /*
  * Standalone row gather and scatter-add.  Replace the reference's

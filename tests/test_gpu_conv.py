@@ -532,7 +532,7 @@ def test_tile_schedule_does_not_change_results(use_sorted):
     x = dev(rng.standard_normal((n, C)).astype(np.float32), torch.bfloat16)
     w = dev(vg.kaiming_uniform(K, 27, C, 11), torch.bfloat16)
     outs, mos = [], []
-    for with_ws in (True, False):
+    for with_ws in (True, False, "given"):
         p = ConvParams(3, ConvOpType.kForward)
         p.conv_algo_desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 32)
         o = torch.full((n, K), float("nan"), dtype=torch.bfloat16, device="cuda")
@@ -544,6 +544,8 @@ def test_tile_schedule_does_not_change_results(use_sorted):
         p.mask_output = mo
         if use_sorted:
             p.indices_sorted = tv.Tensor(pt.sorted_indices("fwd"))
+        if with_ws == "given":
+            p.tile_order = tv.Tensor(pt.tile_order("fwd"))
         if with_ws:
             ConvMainUnitTest(sync_check=True).implicit_gemm2(p)
         else:
@@ -555,10 +557,59 @@ def test_tile_schedule_does_not_change_results(use_sorted):
         outs.append(o.float().cpu())
         mos.append(mo.numpy().copy())
     assert not torch.isnan(outs[0]).any()
-    assert torch.equal(outs[0], outs[1])
-    assert np.array_equal(mos[0], mos[1])
+    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])
+    assert np.array_equal(mos[0], mos[1]) and np.array_equal(mos[0], mos[2])
     m = pt.masks_fwd[0].cpu().numpy().view(np.uint32)
     order = pt.argsorts_fwd[0].cpu().numpy()
     ref, mo_ref = co.conv_fwd_masked(to64(x), to64(w), pt.pairs_fwd.cpu().numpy(), m, order, 32)
     _assert_close(outs[0].double().numpy(), ref, TOL_16)
     assert np.array_equal(mos[0], mo_ref)
+
+
+
+def test_tile_order_is_largest_first_permutation():
+    """SpconvOps.tile_order: a permutation of the 128-row tiles with their
+    offset counts (popcount of the OR-ed masks, mask_filter applied)
+    non-increasing; the reverse (backward-input) count gives the same counts
+    for kv-bit masks; a ragged last tile and a split filter included."""
+    from cumm.spconv_ops import SpconvOps
+    for n, filt in ((30001, 0xffffffff), (5000, 0x3fff), (77, 0xffffffff)):
+        coords, pf, pb, m = _subm(n, 40 if n > 1000 else 8, n)
+        ms, order = po.sort_by_key_split(m, 0xffffffff)
+        md = torch.from_numpy(ms.view(np.int32)).cuda()
+        tiles = (n + 127) // 128
+        pc = np.array([bin(int(np.bitwise_or.reduce(ms[t * 128:(t + 1) * 128])) & filt).count("1")
+                       for t in range(tiles)])
+        for rev in (False, True):
+            o = SpconvOps.tile_order(md, 27, filt, rev).cpu().numpy()
+            assert sorted(o.tolist()) == list(range(tiles))
+            assert np.all(np.diff(pc[o]) <= 0), (n, rev)
+
+
+def test_tile_order_bad_entry_reported():
+    """A caller-supplied tile_order entry outside the row tiles sets the
+    bad-index bit (reported as a device error) instead of being followed."""
+    import torch as _t
+    from cumm.conv.main import ConvMainUnitTest
+    from cumm.spconv_ops import build_pair_table
+    from cumm.tensorview.gemm import ConvParams
+    n, C, K = 4000, 64, 64
+    coords = vg.lidar_voxels(n, seed=3)
+    pt = build_pair_table(_t.from_numpy(coords).cuda(), vg.KITTI_SHAPE)
+    x = dev(np.random.default_rng(3).standard_normal((n, C)).astype(np.float32), torch.bfloat16)
+    w = dev(vg.kaiming_uniform(K, 27, C, 3), torch.bfloat16)
+    for use_sorted in (True, False):
+        p = ConvParams(3, ConvOpType.kForward)
+        p.conv_algo_desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.bfloat16, 128)
+        o = torch.zeros((n, K), dtype=torch.bfloat16, device="cuda")
+        p.input, p.weight, p.output = tv.Tensor(x), tv.Tensor(w), tv.Tensor(o)
+        p.indices = tv.Tensor(pt.pairs_fwd)
+        p.mask = tv.Tensor(pt.masks_fwd[0], tv.uint32)
+        p.mask_argsort = tv.Tensor(pt.argsorts_fwd[0])
+        if use_sorted:
+            p.indices_sorted = tv.Tensor(pt.sorted_indices("fwd"))
+        bad = pt.tile_order("fwd").clone()
+        bad[3] = -5
+        p.tile_order = tv.Tensor(bad)
+        with pytest.raises(RuntimeError, match="device error"):
+            ConvMainUnitTest(sync_check=True).implicit_gemm2(p)

@@ -166,3 +166,20 @@ def test_ops_need_cuda_no_cpu_fallback():
     p = ConvParams(3, ConvOpType.kForward)
     with pytest.raises(RuntimeError, match="CUDA device"):
         ConvMainUnitTest().implicit_gemm2(p)
+
+
+
+def test_tile_order_entry_validation():
+    """sc_tile_order_workspace_size and the argument checks of sc_tile_order
+    (made before any device call)."""
+    lib = _lib.load()
+    n = ctypes.c_int64(-1)
+    assert lib.sc_tile_order_workspace_size(1000, ctypes.byref(n)) == 0 and n.value == 256 + 256
+    assert lib.sc_tile_order_workspace_size(200000, ctypes.byref(n)) == 0
+    assert n.value == 256 + ((1563 * 4 + 255) // 256) * 256
+    assert lib.sc_tile_order_workspace_size(-1, ctypes.byref(n)) == _lib.SC_INVALID_ARG
+    assert lib.sc_tile_order(None, 1000, 0xffffffff, 27, 0, 0x1000, 0x2000, 4096, None) == _lib.SC_INVALID_ARG
+    assert lib.sc_tile_order(0x1000, 1000, 0xffffffff, 40, 0, 0x1000, 0x2000, 4096, None) == _lib.SC_INVALID_ARG
+    rc = lib.sc_tile_order(0x1000, 1000, 0xffffffff, 27, 0, 0x3000, 0x2000, 100, None)
+    assert rc == _lib.SC_RUNTIME and "workspace at least" in lib.sc_last_error().decode()
+    assert lib.sc_tile_order(None, 0, 0xffffffff, 27, 0, None, None, 0, None) == 0
