@@ -170,6 +170,9 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
   constexpr int kTabF = Layout<kPair>::kTabF;
   constexpr int kFStride = Layout<kPair>::kFStride;
   constexpr int kNQ = Layout<kPair>::kNQ;
+  // producer rings: the pair layout's epilogue warps are the second ring's
+  // producers until the mainloop ends
+  constexpr int kRings = kPair ? 2 : 1;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_u32 = smem_u32(smem_raw);
   const uint32_t pad = (1024u - (raw_u32 & 1023u)) & 1023u;
@@ -233,6 +236,101 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
+
+  // ---------------------------------------------------------------- TMA gather producer loop
+  // Producer warps of ring `ring` serve every stage of that ring: warp pw
+  // owns rows [kRpw pw, kRpw pw + kRpw) of each 64-row atom; lane l < 2 kGpw
+  // issues one tile::gather4 for rows kRpw pw + 4 (l % kGpw) .. +3 of atom
+  // l / kGpw (input rows of the atom's filter; a group of four absent rows
+  // reads the zero tensor).  The chunk's 64 dOut rows are the same for every
+  // M-tile, so they are gathered once per chunk into one of the ring's dOut
+  // buffers (lanes l < kGpw n_b_atoms, same row split), released by the MMA
+  // after the chunk's last tile.  Lane 0 of each warp arrives with
+  // expect_tx for its bytes.  With two rings (pair layout) ring r takes the
+  // CTA's chunks it = r, r + 2, ... (index buffers it % 4: 0 and 2 for ring
+  // 0, 1 and 3 for ring 1), and owns half of the stages and dOut buffers.
+  auto produce_gather = [&](int pw, int ring) {
+    constexpr int kRpw = kRows / kProdWarps;  // rows per warp: 8 single, 16 pair
+    constexpr int kGpw = kRpw / 4;            // gathers per atom per warp
+    const int n_b_atoms = P.n_mma / 64;
+    const uint32_t Sr = static_cast<uint32_t>(S / kRings);
+    const uint32_t NBr = P.n_bbuf / kRings;
+    const int rq = pw * kRpw + (lane % kGpw) * 4;
+    uint32_t stage = 0, eph = 0, bb = 0, bph = 0;  // this ring's stage / dOut buffer and phases
+    bool ok = true;
+    int it = ring;
+    for (int c = c_begin + ring * c_step; c < c_end && ok; c += kRings * c_step, it += kRings) {
+      const int b = it % kIdxStages;
+      const uint32_t ph = (it / kIdxStages) & 1;
+      if (!__all_sync(0xffffffffu, mbar_wait(&idx_full[b], ph, abort_flag))) {
+        if (lane == 0) flag_error(A.err, kErrWaitTimeout);
+        break;
+      }
+      const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
+      const int *tab = reinterpret_cast<const int *>(buf);
+      const int *sig_tab = tab + kTabF * kRows;
+      const WMeta *meta = reinterpret_cast<const WMeta *>(sig_tab + kRows);
+      uint32_t bits = meta->active_bits;
+      if (bits) {
+        const uint32_t bi = static_cast<uint32_t>(ring) * NBr + bb;
+        if (!__all_sync(0xffffffffu, mbar_wait(&bempty[bi], bph ^ 1u, abort_flag))) {
+          if (lane == 0) flag_error(A.err, kErrWaitTimeout);
+          break;
+        }
+        if (lane == 0) mbar_arrive_expect_tx(&bfull[bi], static_cast<uint32_t>(n_b_atoms * kRpw) * 128u);
+        __syncwarp();
+        if (lane < kGpw * n_b_atoms) {
+          const int na = lane / kGpw;
+          const int4 q = *reinterpret_cast<const int4 *>(sig_tab + rq);
+          const uint32_t dst = smem_base + P.bbuf_off + bi * (n_b_atoms * 8192u) + na * 8192u + rq * 128;
+          if (P.zero_ok && (q.x & q.y & q.z & q.w) == -1) {
+            const int z = zero_group(blockIdx.x * 64 + pw * 8 + lane, static_cast<uint32_t>(it));
+            tma_gather4(dst, &P.tmap_zero, 0, z, z + 1, z + 2, z + 3, &bfull[bi]);
+          }
+          else
+            tma_gather4(dst, &P.tmap_dout, na * 64, q.x, q.y, q.z, q.w, &bfull[bi]);
+        }
+        if (++bb == NBr) {
+          bb = 0;
+          bph ^= 1u;
+        }
+      }
+      while (bits) {
+        const int jt = __ffs(bits) - 1;
+        bits &= bits - 1;
+        const int tt = t0 + jt;
+        const uint32_t s = static_cast<uint32_t>(ring) * Sr + stage;
+        if (!__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], eph ^ 1, abort_flag))) {
+          if (lane == 0) flag_error(A.err, kErrWaitTimeout);
+          ok = false;
+          break;
+        }
+        if (++stage == Sr) {
+          stage = 0;
+          eph ^= 1u;
+        }
+        if (lane == 0) mbar_arrive_expect_tx(&full_bar[s], 2u * kRpw * 128u);
+        __syncwarp();
+        if (lane < 2 * kGpw) {
+          const int a = 2 * tt + lane / kGpw;
+          const int k = a / P.cpa;
+          int4 q = make_int4(-1, -1, -1, -1);
+          if (a < P.n_atoms && k < A.kv)
+            q = *reinterpret_cast<const int4 *>(tab + (k - k_lo) * kRows + rq);
+          const uint32_t dst = smem_base + s * P.stage_bytes + (lane / kGpw) * 8192u + rq * 128;
+          if (P.zero_ok && (q.x & q.y & q.z & q.w) == -1) {
+            const int z = zero_group(blockIdx.x * 64 + pw * 8 + lane, s + static_cast<uint32_t>(it));
+            tma_gather4(dst, &P.tmap_zero, 0, z, z + 1, z + 2, z + 3, &full_bar[s]);
+          }
+          else
+            tma_gather4(dst, &P.tmap_in, (a % P.cpa) * 64, q.x, q.y, q.z, q.w, &full_bar[s]);
+        }
+      }
+      if (!ok) break;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&idx_empty[b]);
+    }
+  };
 
   if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
     // ---------------------------------------------------------------- index loaders
@@ -340,92 +438,7 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
     // cp.async (src-size 0, no memory request).
     const int pw = warp - kProdWarp0;
     if constexpr (kGather) {
-    // TMA gather: all kProdWarps warps serve every stage.  Warp pw owns rows
-    // [kRpw pw, kRpw pw + kRpw) of each 64-row atom; lane l < 2 kGpw issues
-    // one tile::gather4 for rows kRpw pw + 4 (l % kGpw) .. +3 of atom
-    // l / kGpw (input rows of the atom's filter; index -1 lands as zeros).
-    // The chunk's 64 dOut rows are the same for every M-tile, so they are
-    // gathered once per chunk into one of n_bbuf dOut buffers (lanes
-    // l < kGpw n_b_atoms, same row split), released by the MMA after the
-    // chunk's last tile.  Lane 0 of each warp arrives with expect_tx for its
-    // bytes.
-    constexpr int kRpw = kRows / kProdWarps;  // rows per warp: 8 single, 16 pair
-    constexpr int kGpw = kRpw / 4;            // gathers per atom per warp
-    const int n_b_atoms = P.n_mma / 64;
-    const int rq = pw * kRpw + (lane % kGpw) * 4;
-    int it = 0;
-    uint32_t stage = 0, eph = 0, bb = 0, bph = 0;  // dOut buffer and its phase
-    bool ok = true;
-    for (int c = c_begin; c < c_end && ok; c += c_step, ++it) {
-      const int b = it % kIdxStages;
-      const uint32_t ph = (it / kIdxStages) & 1;
-      if (!__all_sync(0xffffffffu, mbar_wait(&idx_full[b], ph, abort_flag))) {
-        if (lane == 0) flag_error(A.err, kErrWaitTimeout);
-        break;
-      }
-      const uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
-      const int *tab = reinterpret_cast<const int *>(buf);
-      const int *sig_tab = tab + kTabF * kRows;
-      const WMeta *meta = reinterpret_cast<const WMeta *>(sig_tab + kRows);
-      uint32_t bits = meta->active_bits;
-      if (bits) {
-        if (!__all_sync(0xffffffffu, mbar_wait(&bempty[bb], bph ^ 1u, abort_flag))) {
-          if (lane == 0) flag_error(A.err, kErrWaitTimeout);
-          break;
-        }
-        if (lane == 0) mbar_arrive_expect_tx(&bfull[bb], static_cast<uint32_t>(n_b_atoms * kRpw) * 128u);
-        __syncwarp();
-        if (lane < kGpw * n_b_atoms) {
-          const int na = lane / kGpw;
-          const int4 q = *reinterpret_cast<const int4 *>(sig_tab + rq);
-          const uint32_t dst = smem_base + P.bbuf_off + bb * (n_b_atoms * 8192u) + na * 8192u + rq * 128;
-          if (P.zero_ok && (q.x & q.y & q.z & q.w) == -1) {
-            const int z = zero_group(blockIdx.x * 64 + pw * 8 + lane, static_cast<uint32_t>(it));
-            tma_gather4(dst, &P.tmap_zero, 0, z, z + 1, z + 2, z + 3, &bfull[bb]);
-          }
-          else
-            tma_gather4(dst, &P.tmap_dout, na * 64, q.x, q.y, q.z, q.w, &bfull[bb]);
-        }
-        if (++bb == P.n_bbuf) {
-          bb = 0;
-          bph ^= 1u;
-        }
-      }
-      while (bits) {
-        const int jt = __ffs(bits) - 1;
-        bits &= bits - 1;
-        const int tt = t0 + jt;
-        const uint32_t s = stage;
-        if (!__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], eph ^ 1, abort_flag))) {
-          if (lane == 0) flag_error(A.err, kErrWaitTimeout);
-          ok = false;
-          break;
-        }
-        if (++stage == static_cast<uint32_t>(S)) {
-          stage = 0;
-          eph ^= 1u;
-        }
-        if (lane == 0) mbar_arrive_expect_tx(&full_bar[s], 2u * kRpw * 128u);
-        __syncwarp();
-        if (lane < 2 * kGpw) {
-          const int a = 2 * tt + lane / kGpw;
-          const int k = a / P.cpa;
-          int4 q = make_int4(-1, -1, -1, -1);
-          if (a < P.n_atoms && k < A.kv)
-            q = *reinterpret_cast<const int4 *>(tab + (k - k_lo) * kRows + rq);
-          const uint32_t dst = smem_base + s * P.stage_bytes + (lane / kGpw) * 8192u + rq * 128;
-          if (P.zero_ok && (q.x & q.y & q.z & q.w) == -1) {
-            const int z = zero_group(blockIdx.x * 64 + pw * 8 + lane, static_cast<uint32_t>(stage + it));
-            tma_gather4(dst, &P.tmap_zero, 0, z, z + 1, z + 2, z + 3, &full_bar[s]);
-          }
-          else
-            tma_gather4(dst, &P.tmap_in, (a % P.cpa) * 64, q.x, q.y, q.z, q.w, &full_bar[s]);
-        }
-      }
-      if (!ok) break;
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&idx_empty[b]);
-    }
+      produce_gather(pw, 0);
     } else {
     const int u = lane & 7;
     const int rg = lane >> 3;
@@ -522,10 +535,18 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
       int it = 0;
+      // stage, full phase, dOut buffer and its phase of the ring of the
+      // current chunk (c) and of the other ring (o); the rings alternate
+      // chunk by chunk, so the two sets swap after every chunk (scalars, so
+      // they stay in registers)
       uint32_t stage = 0, fph = 0, bb = 0, bph = 0;
+      uint32_t stage_o = 0, fph_o = 0, bb_o = 0, bph_o = 0;
+      const uint32_t Sr = static_cast<uint32_t>(S / kRings);
+      const uint32_t NBr = P.n_bbuf / kRings;
       uint32_t started = 0;
       bool ok = true;
       for (int c = c_begin; c < c_end && ok; c += c_step, ++it) {
+        const int ring = kRings == 2 ? (it & 1) : 0;
         const int b = it % kIdxStages;
         const uint32_t ph = (it / kIdxStages) & 1;
         if (!mbar_wait(&idx_full[b], ph, abort_flag)) {
@@ -538,17 +559,18 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
         mbar_arrive(&idx_empty[b]);
         uint32_t sBg = 0;
         const bool chunk_used = bits != 0;
+        const uint32_t bi = static_cast<uint32_t>(ring) * NBr + bb;
         if (kGather && chunk_used) {
-          if (!mbar_wait(&bfull[bb], bph, abort_flag)) {
+          if (!mbar_wait(&bfull[bi], bph, abort_flag)) {
             flag_error(A.err, kErrWaitTimeout);
             break;
           }
-          sBg = smem_base + P.bbuf_off + bb * ((P.n_mma / 64) * 8192u);
+          sBg = smem_base + P.bbuf_off + bi * ((P.n_mma / 64) * 8192u);
         }
         while (bits) {
           const int j = __ffs(bits) - 1;
           bits &= bits - 1;
-          const uint32_t s = stage;
+          const uint32_t s = static_cast<uint32_t>(ring) * Sr + stage;
           if (!mbar_wait(&full_bar[s], fph, abort_flag)) {
             flag_error(A.err, kErrWaitTimeout);
             ok = false;
@@ -567,17 +589,24 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
           }
           started |= 1u << j;
           mma_commit(&empty_bar[s]);
-          if (++stage == static_cast<uint32_t>(S)) {
+          if (++stage == Sr) {
             stage = 0;
             fph ^= 1u;
           }
         }
         if (kGather && chunk_used && ok) {
-          mma_commit(&bempty[bb]);  // dOut buffer free once these MMAs finish
-          if (++bb == P.n_bbuf) {
+          mma_commit(&bempty[bi]);  // dOut buffer free once these MMAs finish
+          if (++bb == NBr) {
             bb = 0;
             bph ^= 1u;
           }
+        }
+        if constexpr (kRings == 2) {
+          uint32_t x;
+          x = stage; stage = stage_o; stage_o = x;
+          x = fph; fph = fph_o; fph_o = x;
+          x = bb; bb = bb_o; bb_o = x;
+          x = bph; bph = bph_o; bph_o = x;
         }
       }
       if (started) {
@@ -602,6 +631,8 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
     // then owns 4 consecutive channels of one column and adds them with one
     // red.global.add.v4.f32 (a quarter of the scalar atomics).  Only
     // __syncwarp is used: a warp whose wait ran out never strands the others.
+    // In the pair layout these warps first produce for the second ring.
+    if constexpr (kGather && kPair) produce_gather(warp, 1);
     if (mbar_wait(acc_full, 0, abort_flag)) {
       tc_fence_after();
       const uint32_t used = *reinterpret_cast<volatile uint32_t *>(used_tiles);
@@ -734,15 +765,16 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t 
     const int64_t st = budget > 0 ? budget / P.stage_bytes : 0;
     return static_cast<int>(st > 8 ? 8 : st);
   };
-  // Two CTAs per SM on the gather path with 64 dOut columns, when three
-  // stages and two dOut buffers fit in 113 KB.
-  const bool pair = gather && P.n_mma == 64 && stages_for(true, 2 * b_bytes) >= 3;
+  // Two CTAs per SM on the gather path with 64 dOut columns, when each of
+  // their two producer rings gets two stages and two dOut buffers in 113 KB.
+  const bool pair = gather && P.n_mma == 64 && stages_for(true, kMaxBBufs * b_bytes) >= 4;
   // The producers can run n_bbuf - 1 chunks ahead of the MMA (a chunk's dOut
   // buffer is released after its last M-tile): four buffers when that still
-  // leaves four stages (three in the pair layout), else two.
-  P.n_bbuf = gather ? (stages_for(pair, kMaxBBufs * b_bytes) >= (pair ? 3 : 4) ? kMaxBBufs : 2) : 1;
+  // leaves four stages, else two (one ring).
+  P.n_bbuf = gather ? (pair || stages_for(false, kMaxBBufs * b_bytes) >= 4 ? kMaxBBufs : 2) : 1;
   const uint32_t bbuf_bytes = gather ? P.n_bbuf * b_bytes : 0;
-  const int stages = stages_for(pair, bbuf_bytes);
+  int stages = stages_for(pair, bbuf_bytes);
+  if (pair) stages &= ~1;  // an equal share per ring
   if (stages < 2) return cudaErrorInvalidConfiguration;
   P.idx_buf_bytes = idx_buf_for(pair);
   // M-tile groups: TMEM columns per CTA (512, or 256 for each of a pair)
