@@ -75,6 +75,7 @@ def run_forward(cfg: FwdConfig, x: torch.Tensor, w: torch.Tensor, out: torch.Ten
         p.mask = tv.Tensor(pt.masks_fwd[j], tv.uint32)
         p.mask_argsort = tv.Tensor(pt.argsorts_fwd[j])
         p.indices_sorted = tv.Tensor(pt.sorted_indices("fwd", j))
+        p.tile_order = tv.Tensor(pt.tile_order("fwd", j))
         p.mask_filter = pt.split_masks[j] if cfg.num_split > 1 else 0xffffffff
         p.beta = 1.0 if j > 0 else 0.0
         p.tile_n = cfg.tile_n
