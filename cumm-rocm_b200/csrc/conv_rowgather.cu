@@ -953,28 +953,32 @@ __global__ void __maxnreg__(kPair ? 80 : 96)
 }
 
 // ------------------------------------------------------------------ strand kernel
-// Forward / backward-input over 128-byte gathered rows with several
+// Forward / backward-input over 128-byte (SWIZZLE_128B) or 64-byte
+// (SWIZZLE_64B: C = 64 e4m3, C = 32 bf16 / f16) gathered rows with several
 // independent pipelines ("strands") per SM: two CTAs per SM, each running
 // kStrands strands.  A strand owns kSProd producer warps, its own ring of
-// kSStages stages (128 gathered rows + the weight slab), one MMA warp and a
-// double-buffered TMEM accumulator; the four epilogue warps of the CTA serve
-// both strands.  Measured on B200: one tcgen05.mma stream (one issuing warp)
+// P.stages stages (128 gathered rows + the weight slab; as many as fit, 2 of
+// 24 KB for 128-byte rows at BN = 64, 4 of 12 KB for 64-byte rows), one MMA
+// warp and a double-buffered TMEM accumulator; the four epilogue warps of the
+// CTA serve both strands.  The kernel is bound by the latency of its rings
+// (each stage needs a producer -> MMA -> producer round trip), so the ring
+// depth that shared memory allows sets its speed.  Measured on B200: one tcgen05.mma stream (one issuing warp)
 // completes an M = 128, K = 16 MMA about every 170 cycles whatever N is, and
 // one producer ring (its warps, stages and barriers) fills ~18-30 bytes per
 // cycle; both rates grow with the number of independent streams on the SM
 // (four MMA warps: ~5450 FLOP/clk/SM at N = 64; four rings of four TMA warps:
-// ~65 B/clk/SM), which the strands provide.  Tiles are dealt round-robin over
-// all strands of the grid.  Every role derives its tiles' masks itself (the
+// ~65 B/clk/SM), which the strands provide.  Tiles are taken in the
+// largest-first order when one is given (strand_tile), else round-robin.  Every role derives its tiles' masks itself (the
 // tile's mask words OR-ed per 32-row group), and the producers read each
 // gather's four indices straight from the sorted index table, so the strands
 // share no index ring.  Needs indices_sorted (16-byte aligned, M % 4 == 0)
 // and BN <= 64.
 constexpr int kStrands = 2;
 constexpr int kSProd = 4;
-constexpr int kSStages = 2;
+constexpr int kSMaxStages = 4;  // stages per strand: 2 of 24 KB (128-byte rows), 4 of 12 KB (64-byte rows)
 constexpr int kSWarps = kEpiWarps + kStrands * (kSProd + 1);  // 14
 constexpr int kSThreads = kSWarps * 32;
-constexpr int kSBars = 2 * kSStages + 7;  // barriers per strand
+constexpr int kSBars = 2 * kSMaxStages + 7;  // barriers per strand
 constexpr uint32_t kSTmemCols = 256;      // per CTA: kStrands x 2 buffers x BN (<= 64)
 
 struct TileMasks {
@@ -1033,7 +1037,7 @@ __device__ __forceinline__ int64_t strand_tile(const KParams &P, int64_t pos, in
   return d < P.num_tiles ? scheduled_tile(P.a, d) : -1;
 }
 
-template <bool kF8, typename TOut>
+template <bool kF8, typename TOut, bool kWide>
 __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KParams P) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_u32 = smem_u32(smem_raw);
@@ -1041,7 +1045,10 @@ __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KPara
   uint8_t *smem = smem_raw + pad;
   const uint32_t smem_base = raw_u32 + pad;
   const ConvRowGatherArgs &A = P.a;
-  constexpr int S = kSStages;
+  // kWide: 128-byte rows (SWIZZLE_128B), two 24 KB stages per strand; else
+  // 64-byte rows (SWIZZLE_64B), four 12 KB stages
+  constexpr int S = kWide ? 2 : 4;
+  constexpr int rb = kWide ? 128 : 64;
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + P.bar_off);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + kStrands * kSBars);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
@@ -1107,9 +1114,9 @@ __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KPara
       // the two chunks before it.
       const int pw = role;
       const int esz = kF8 ? 1 : 2;
-      const int box = 128 / esz;
-      const uint32_t a_tx = 32u * 128u;
-      const uint32_t b_tx = static_cast<uint32_t>(A.BN) * 128u;
+      const int box = rb / esz;
+      const uint32_t a_tx = 32u * static_cast<uint32_t>(rb);
+      const uint32_t b_tx = static_cast<uint32_t>(A.BN) * static_cast<uint32_t>(rb);
       const int r0 = pw * 32 + lane * 4;
       // cursor (warp-uniform): tile (the strand's c_it-th), offsets not
       // started yet, current offset / column block
@@ -1228,10 +1235,10 @@ __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KPara
           }
           if (P.zero_ok && (q0.x & q0.y & q0.z & q0.w) == -1) {
             const int z = zero_group(blockIdx.x * 64 + warp * 8 + lane, gchunk);
-            tma_gather4(sA + r0 * 128, &P.tmap_zero, 0, z, z + 1, z + 2, z + 3, &full[stage]);
+            tma_gather4(sA + r0 * rb, &P.tmap_zero, 0, z, z + 1, z + 2, z + 3, &full[stage]);
           }
           else
-            tma_gather4(sA + r0 * 128, &P.tmap_a, cb0 * box, q0.x, q0.y, q0.z, q0.w, &full[stage]);
+            tma_gather4(sA + r0 * rb, &P.tmap_a, cb0 * box, q0.x, q0.y, q0.z, q0.w, &full[stage]);
         }
         ++gchunk;
         if (++stage == static_cast<uint32_t>(S)) {
@@ -1244,6 +1251,11 @@ __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KPara
     } else {
       // ---------------------------------------------------------------- MMA warp
       const uint64_t b_kstep = P.b_mn ? 128 : 2;
+      // 8-row swizzle atoms 1024 bytes apart (SWIZZLE_128B) or 512 (SWIZZLE_64B);
+      // one MMA per 32 bytes of K
+      constexpr uint32_t sbo = kWide ? 1024u : 512u;
+      constexpr uint32_t swz = kWide ? 2u : 4u;
+      constexpr int mmas = rb / 32;
       uint32_t stage = 0, fph = 0;
       bool issued = false, ok = true;
       for (int it = 0;; ++it) {
@@ -1277,10 +1289,11 @@ __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KPara
                 }
                 tc_fence_after();
                 const uint32_t sA = ring + stage * P.stage_bytes;
-                const uint64_t ad = make_sdesc(sA, 16, 1024);
-                const uint64_t bd = P.b_mn ? make_sdesc(sA + P.b_off, 8192, 1024) : make_sdesc(sA + P.b_off, 16, 1024);
+                const uint64_t ad = make_sdesc_l(sA, 16, sbo, swz);
+                const uint64_t bd = P.b_mn ? make_sdesc(sA + P.b_off, 8192, 1024)
+                                           : make_sdesc_l(sA + P.b_off, 16, sbo, swz);
 #pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
+                for (int kk = 0; kk < mmas; ++kk) {
                   if constexpr (kF8)
                     mma_f8(d, ad + static_cast<uint64_t>(kk * 2), bd + static_cast<uint64_t>(kk) * b_kstep, P.idesc,
                            (j | kk) != 0 ? 1u : 0u);
@@ -1394,7 +1407,8 @@ __global__ void __maxnreg__(72) conv_strand_kernel(const __grid_constant__ KPara
 
 template <bool kF8, typename TOut>
 cudaError_t launch_strands(const KParams &P, int grid, size_t smem, cudaStream_t stream) {
-  void (*kern)(KParams) = conv_strand_kernel<kF8, TOut>;
+  void (*kern)(KParams) = P.row_bytes == 128 ? conv_strand_kernel<kF8, TOut, true>
+                                             : conv_strand_kernel<kF8, TOut, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   kern<<<grid, kSThreads, smem, stream>>>(P);
@@ -1516,11 +1530,14 @@ cudaError_t launch_conv_rowgather(const ConvRowGatherArgs &a, int num_sms, cudaS
   // Strands (two independent pipelines per CTA, two CTAs per SM) on the TMA
   // gather path of 128-byte rows with the sorted index table and BN <= 64
   // (TMEM: 2 strands x 2 buffers x BN columns per CTA).
-  if (gather && P.row_bytes == 128 && P.bulk_idx && a.BN <= 64) {
+  if (gather && P.bulk_idx && a.BN <= 64 && !(P.row_bytes == 64 && a.b_mn)) {
     if (P.num_tiles == 0) return cudaSuccess;
-    P.stages = kSStages;
+    // two CTAs per SM (113 KB each): two stages per strand with 128-byte rows
+    // (24 KB at BN 64), four with 64-byte rows (12 KB)
+    const int stages = P.row_bytes == 128 ? 2 : 4;
+    P.stages = stages;
     P.tmem_cols = kSTmemCols;
-    P.bar_off = P.stage_bytes * kStrands * kSStages;
+    P.bar_off = P.stage_bytes * kStrands * stages;
     const size_t smem = 1024 + P.bar_off + 512;
     const int64_t ctas = (P.num_tiles + kStrands - 1) / kStrands;
     const int grid = static_cast<int>(ctas < 2 * num_sms ? ctas : 2 * num_sms);

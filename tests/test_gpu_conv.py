@@ -444,7 +444,9 @@ def test_sorted_index_table_identical(n):
 @pytest.mark.parametrize("n,grid,C,K,tile_n,tile_m", [
     (4000, 24, 64, 64, 0, 128), (4000, 24, 64, 64, 32, 64), (4000, 24, 64, 64, 16, 32),
     (2000, 20, 128, 64, 0, 128), (2000, 20, 64, 128, 64, 128), (2000, 20, 128, 128, 64, 32),
-    (4, 8, 64, 64, 0, 128), (132, 10, 64, 64, 0, 128)])
+    (4, 8, 64, 64, 0, 128), (132, 10, 64, 64, 0, 128),
+    # 64-byte rows (SWIZZLE_64B stages, four per strand): C = 32 forward, K = 32 backward-input
+    (4000, 24, 32, 32, 0, 128), (4000, 24, 32, 64, 32, 64), (3000, 20, 64, 32, 16, 32), (132, 10, 32, 32, 0, 128)])
 def test_strand_kernel_shapes(n, grid, C, K, tile_n, tile_m):
     """Forward and backward-input through the strand kernel (sorted index
     table, 128-byte rows, column tiles <= 64): several chunks per offset
@@ -613,3 +615,32 @@ def test_tile_order_bad_entry_reported():
         p.tile_order = tv.Tensor(bad)
         with pytest.raises(RuntimeError, match="device error"):
             ConvMainUnitTest(sync_check=True).implicit_gemm2(p)
+
+
+
+@pytest.mark.parametrize("n,K,tile_m", [(6000, 64, 128), (2000, 128, 32), (132, 64, 128)])
+def test_strand_kernel_e4m3_64byte_rows(n, K, tile_m):
+    """E4M3 with C = 64 (64-byte rows): the strand kernel with SWIZZLE_64B
+    stages (four per strand), per-output-channel scale epilogue, several column
+    tiles (K = 128), mask_output, against the FP64 oracle on the rounded
+    operands."""
+    C = 64
+    coords, pf, pb, m = _subm(n, 26 if n > 1000 else 10, n + 3)
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal((n, C)).astype(np.float32)
+    w = vg.kaiming_uniform(K, 27, C, n)
+    sx = np.abs(x).max() / 448.0
+    sw = np.abs(w).reshape(K, -1).max(1) / 448.0
+    xq = dev(x / sx, torch.float8_e4m3fn)
+    wq = dev(w / sw[:, None, None], torch.float8_e4m3fn)
+    scale = dev((sx * sw).astype(np.float32))
+    ms, order = po.sort_by_key_split(m, 0xffffffff)
+    out = torch.zeros((n, K), dtype=torch.bfloat16, device="cuda")
+    mo = tv.zeros([(n + tile_m - 1) // tile_m], tv.uint32, 0)
+    desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.float_e4m3, tv.float_e4m3, tv.bfloat16, tile_m)
+    conv(ConvOpType.kForward, desp, xq, wq, out, pf, ms, order, scale=scale, sorted_indices=True,
+         mask_output=mo, tile_n=64 if K > 64 else 0)
+    ref, mo_ref = co.conv_fwd_masked(to64(xq), to64(wq), pf, ms, order, tile_m,
+                                     scale=(sx * sw).astype(np.float64))
+    _assert_close(to64(out), ref, TOL_16)
+    assert np.array_equal(mo.numpy(), mo_ref)
