@@ -59,6 +59,17 @@ class SparseEncoder:
         self.wq: List[torch.Tensor] = []
         self.sw: List[torch.Tensor] = []
         self.sx: List[torch.Tensor] = []
+        self._streams: List[torch.cuda.Stream] = []
+
+    def streams(self, n: int) -> List[torch.cuda.Stream]:
+        """The encoder's first n pass streams, created once and reused by every
+        serve() call: the caching allocator keeps freed blocks per stream, so
+        a warm-up on these streams leaves exactly their pools holding the
+        buffers of full-size passes (fresh streams would allocate, and near
+        the device limit free and re-allocate, on the host during the run)."""
+        while len(self._streams) < n:
+            self._streams.append(torch.cuda.Stream(device=self.dev))
+        return self._streams[:n]
 
     def calibrate(self, coords: torch.Tensor, feats: torch.Tensor):
         """Fixes the E4M3 activation tile scales from one bf16 pass (amax of
@@ -211,7 +222,7 @@ def serve(enc: SparseEncoder, requests: List[Request], continuous: bool = True,
     t0 = time.perf_counter()
     batches = []
     if not continuous:
-        s = torch.cuda.Stream()
+        s = enc.streams(1)[0]
         for r in reqs:
             now = time.perf_counter() - t0
             if now < r.arrival:
@@ -222,7 +233,7 @@ def serve(enc: SparseEncoder, requests: List[Request], continuous: bool = True,
     else:
         adm = Admission(budget_bytes, slots)
         queue = deque(reqs)
-        free_streams = deque(torch.cuda.Stream() for _ in range(slots))
+        free_streams = deque(enc.streams(slots))
         lock = threading.Lock()
         threads, errors = [], []
 
