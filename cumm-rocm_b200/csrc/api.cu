@@ -194,6 +194,9 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
         return fail(SC_INVALID_ARG, "%s must start on a 16-byte boundary for the tcgen05 kernels (address %p)",
                     names[i], need[i]);
   }
+  if (reinterpret_cast<uintptr_t>(p->tile_order) % 4 != 0)
+    return fail(SC_INVALID_ARG, "tile_order must be 4-byte aligned (address %p)",
+                static_cast<const void *>(p->tile_order));
   if (p->tile_n != 0 && op != SC_CONV_BACKWARD_WEIGHT) {
     const int64_t ncols = op == SC_CONV_FORWARD ? p->K : p->C;
     if (p->tile_n < 16 || p->tile_n > 256 || p->tile_n % 16 || ncols % p->tile_n)

@@ -183,3 +183,12 @@ def test_tile_order_entry_validation():
     rc = lib.sc_tile_order(0x1000, 1000, 0xffffffff, 27, 0, 0x3000, 0x2000, 100, None)
     assert rc == _lib.SC_RUNTIME and "workspace at least" in lib.sc_last_error().decode()
     assert lib.sc_tile_order(None, 0, 0xffffffff, 27, 0, None, None, 0, None) == 0
+
+
+
+def test_misaligned_tile_order_rejected():
+    """A tile_order that is not 4-byte aligned is an argument error before any
+    launch (the kernels read it as int32)."""
+    rc, _, msg = _ws(_fake_conv(0, tile_order=0x1002))
+    assert rc == _lib.SC_INVALID_ARG and "tile_order" in msg
+    assert _ws(_fake_conv(0, tile_order=0x1004))[0] == 0
