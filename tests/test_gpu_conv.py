@@ -644,3 +644,78 @@ def test_strand_kernel_e4m3_64byte_rows(n, K, tile_m):
                                      scale=(sx * sw).astype(np.float64))
     _assert_close(to64(out), ref, TOL_16)
     assert np.array_equal(mo.numpy(), mo_ref)
+
+
+def test_tile_order_backward_input_and_split_masks():
+    """The largest-first order made for the forward masks serves the
+    submanifold backward-input (reverse_mask) and each mask split of the
+    MaskSplitImplicitGemm form: results are bit-identical to calls that get a
+    workspace but no order (each computes the order itself) and match the FP64
+    oracle."""
+    import ctypes
+    from cumm import _lib
+    from cumm.conv.main import ConvMainUnitTest, build_conv_params_c
+    from cumm.spconv_ops import build_pair_table
+    from cumm.tensorview.gemm import ConvParams
+    n, C, K = 36000, 64, 64
+    coords = vg.lidar_voxels(n, seed=21)
+    pt = build_pair_table(torch.from_numpy(coords).cuda(), vg.KITTI_SHAPE, num_split=2)
+    rng = np.random.default_rng(21)
+    w = dev(vg.kaiming_uniform(K, 27, C, 21), torch.bfloat16)
+    dy = dev(rng.standard_normal((n, K)).astype(np.float32), torch.bfloat16)
+    x = dev(rng.standard_normal((n, C)).astype(np.float32), torch.bfloat16)
+
+    def call(p, given):
+        if given:
+            ConvMainUnitTest(sync_check=True).implicit_gemm2(p)
+        else:
+            cp, _info = build_conv_params_c(p)
+            cp.flags |= _lib.SC_FLAG_SYNC_CHECK
+            cp.tile_order = None
+            lib = _lib.load()
+            need = ctypes.c_int64(0)
+            _lib.check(lib.sc_conv_workspace_size(ctypes.byref(cp), ctypes.byref(need)))
+            ws = torch.empty(max(need.value, 256), dtype=torch.uint8, device="cuda")
+            # a workspace but no order: the call orders the tiles itself
+            cp.workspace, cp.workspace_bytes = ws.data_ptr(), ws.numel()
+            _lib.check(lib.sc_conv_implicit_gemm(ctypes.byref(cp)))
+        torch.cuda.synchronize()
+
+    dins, outs = [], []
+    for given in (True, False):
+        din = torch.zeros((n, C), dtype=torch.bfloat16, device="cuda")
+        out = torch.zeros((n, K), dtype=torch.float32, device="cuda")
+        for j in range(2):
+            p = ConvParams(3, ConvOpType.kBackwardInput)
+            p.conv_algo_desp = find_desp(ConvOpType.kBackwardInput, "Tcgen05", tv.bfloat16, tv.bfloat16,
+                                         tv.bfloat16, 128)
+            p.input, p.weight, p.output = tv.Tensor(din), tv.Tensor(w), tv.Tensor(dy)
+            p.indices = tv.Tensor(pt.pairs_bwd)
+            p.mask = tv.Tensor(pt.masks_fwd[j], tv.uint32)
+            p.mask_argsort = tv.Tensor(pt.argsorts_fwd[j])
+            p.indices_sorted = tv.Tensor(pt.sorted_indices("bwd", j))
+            p.reverse_mask = True
+            p.mask_filter = pt.split_masks[j]
+            p.beta = 1.0 if j else 0.0
+            if given:
+                p.tile_order = tv.Tensor(pt.tile_order("bwd", j))
+            call(p, given)
+            q = ConvParams(3, ConvOpType.kForward)
+            q.conv_algo_desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.float32, 128)
+            q.input, q.weight, q.output = tv.Tensor(x), tv.Tensor(w), tv.Tensor(out)
+            q.indices = tv.Tensor(pt.pairs_fwd)
+            q.mask = tv.Tensor(pt.masks_fwd[j], tv.uint32)
+            q.mask_argsort = tv.Tensor(pt.argsorts_fwd[j])
+            q.indices_sorted = tv.Tensor(pt.sorted_indices("fwd", j))
+            q.mask_filter = pt.split_masks[j]
+            q.beta = 1.0 if j else 0.0
+            if given:
+                q.tile_order = tv.Tensor(pt.tile_order("fwd", j))
+            call(q, given)
+        dins.append(din.float().cpu())
+        outs.append(out.cpu())
+    assert torch.equal(dins[0], dins[1])
+    assert torch.equal(outs[0], outs[1])
+    pf, pb = pt.pairs_fwd.cpu().numpy(), pt.pairs_bwd.cpu().numpy()
+    _assert_close(dins[0].double().numpy(), co.dgrad_gather_gemm_scatter(to64(dy), to64(w), pb), TOL_16)
+    _assert_close(outs[0].double().numpy(), co.fwd_gather_gemm_scatter(to64(x), to64(w), pf), TOL_16)
