@@ -717,5 +717,8 @@ def test_tile_order_backward_input_and_split_masks():
     assert torch.equal(dins[0], dins[1])
     assert torch.equal(outs[0], outs[1])
     pf, pb = pt.pairs_fwd.cpu().numpy(), pt.pairs_bwd.cpu().numpy()
-    _assert_close(dins[0].double().numpy(), co.dgrad_gather_gemm_scatter(to64(dy), to64(w), pb), TOL_16)
+    # the split backward-input writes bf16 dIn twice (the second launch adds
+    # to the rounded first half), so it carries two bf16 roundings: twice the
+    # one-launch tolerance; the forward accumulates into fp32
+    _assert_close(dins[0].double().numpy(), co.dgrad_gather_gemm_scatter(to64(dy), to64(w), pb), 2 * TOL_16)
     _assert_close(outs[0].double().numpy(), co.fwd_gather_gemm_scatter(to64(x), to64(w), pf), TOL_16)
