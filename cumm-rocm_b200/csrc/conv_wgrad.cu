@@ -332,6 +332,54 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
     }
   };
 
+  // ---------------------------------------------------------------- dW reduction
+  // TMEM lane m holds M element m of every tile; the warp that reads lane
+  // quadrant q (lanes 32 q .. 32 q + 31) turns its 32 lanes x 32 columns
+  // through a private shared-memory tile (the stage buffers are idle once the
+  // MMA warp drained), so that a lane then owns 4 consecutive channels of one
+  // column and adds them with one red.global.add.v4.f32 (a quarter of the
+  // scalar atomics).  It reduces the CTA's used tiles j = j0, j0 + jstep, ...;
+  // in the pair layout the epilogue warps take the even tiles and ring 0's
+  // producer warps (same quadrants, idle once their ring is done) the odd ones.
+  // Only __syncwarp is used: a warp whose wait ran out never strands the others.
+  auto reduce_tiles = [&](int q, int j0, int jstep) {
+    if (!mbar_wait(acc_full, 0, abort_flag)) {
+      flag_error(A.err, kErrWaitTimeout);
+      return;
+    }
+    tc_fence_after();
+    const uint32_t used = *reinterpret_cast<volatile uint32_t *>(used_tiles);
+    const uint32_t lane_base = static_cast<uint32_t>(q * 32) << 16;
+    float *tb = reinterpret_cast<float *>(smem) + warp * (32 * 33);
+    const int h = q >> 1;               // atom of this warp's 32 M elements
+    const int e_base = (q & 1) * 32;    // first element of the warp inside the atom
+    for (int j = j0; j < t1 - t0; j += jstep) {
+      if (!((used >> j) & 1u)) continue;
+      const int a = 2 * (t0 + j) + h;
+      for (int n0 = 0; n0 < P.n_mma; n0 += 32) {
+        float v[32];
+        tmem_ld32(tmem_base + lane_base + static_cast<uint32_t>(j * P.n_mma + n0), v);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) tb[i * 33 + lane] = v[i];
+        __syncwarp();
+        const int n = n0 + lane;
+        if (a < P.n_atoms && n < A.K) {
+#pragma unroll
+          for (int qq = 0; qq < 8; ++qq) {
+            int k = 0, ch = 0;
+            atom_elem(P, a, e_base + 4 * qq, k, ch);
+            if (k < A.kv && ((A.mask_filter >> k) & 1u)) {
+              const float *src = tb + lane * 33 + 4 * qq;
+              red_add_v4(A.ws + (static_cast<int64_t>(n) * A.kv + k) * A.C + ch, src[0], src[1], src[2],
+                         src[3]);
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+  };
+
   if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
     // ---------------------------------------------------------------- index loaders
     const int t = threadIdx.x - kLoadWarp0 * 32;
@@ -439,6 +487,7 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
     const int pw = warp - kProdWarp0;
     if constexpr (kGather) {
       produce_gather(pw, 0);
+      if constexpr (kPair) reduce_tiles(pw, 1, 2);
     } else {
     const int u = lane & 7;
     const int rg = lane >> 3;
@@ -625,49 +674,9 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
     }
   } else if (warp < kEpiWarps) {
     // ---------------------------------------------------------------- epilogue (warps 0-3)
-    // TMEM lane m (= threadIdx.x) holds M element m of every tile; each warp
-    // turns its 32 lanes x 32 columns through a private shared-memory tile
-    // (the stage buffers are idle once the MMA warp drained), so that a lane
-    // then owns 4 consecutive channels of one column and adds them with one
-    // red.global.add.v4.f32 (a quarter of the scalar atomics).  Only
-    // __syncwarp is used: a warp whose wait ran out never strands the others.
     // In the pair layout these warps first produce for the second ring.
     if constexpr (kGather && kPair) produce_gather(warp, 1);
-    if (mbar_wait(acc_full, 0, abort_flag)) {
-      tc_fence_after();
-      const uint32_t used = *reinterpret_cast<volatile uint32_t *>(used_tiles);
-      const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
-      float *tb = reinterpret_cast<float *>(smem) + warp * (32 * 33);
-      const int h = warp >> 1;               // atom of this warp's 32 M elements
-      const int e_base = (warp & 1) * 32;    // first element of the warp inside the atom
-      for (int j = 0; j < t1 - t0; ++j) {
-        if (!((used >> j) & 1u)) continue;
-        const int a = 2 * (t0 + j) + h;
-        for (int n0 = 0; n0 < P.n_mma; n0 += 32) {
-          float v[32];
-          tmem_ld32(tmem_base + lane_base + static_cast<uint32_t>(j * P.n_mma + n0), v);
-#pragma unroll
-          for (int i = 0; i < 32; ++i) tb[i * 33 + lane] = v[i];
-          __syncwarp();
-          const int n = n0 + lane;
-          if (a < P.n_atoms && n < A.K) {
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              int k = 0, ch = 0;
-              atom_elem(P, a, e_base + 4 * q, k, ch);
-              if (k < A.kv && ((A.mask_filter >> k) & 1u)) {
-                const float *src = tb + lane * 33 + 4 * q;
-                red_add_v4(A.ws + (static_cast<int64_t>(n) * A.kv + k) * A.C + ch, src[0], src[1],
-                           src[2], src[3]);
-              }
-            }
-          }
-          __syncwarp();
-        }
-      }
-    } else {
-      flag_error(A.err, kErrWaitTimeout);
-    }
+    reduce_tiles(warp, 0, kPair ? 2 : 1);
   }
 
   tc_fence_before();
