@@ -362,16 +362,24 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
 #pragma unroll
         for (int i = 0; i < 32; ++i) tb[i * 33 + lane] = v[i];
         __syncwarp();
-        const int n = n0 + lane;
-        if (a < P.n_atoms && n < A.K) {
+        // lane = (channel quad c4, column nsub): the 8 lanes of one column
+        // cover the warp's 32 consecutive channels, so each instruction adds
+        // 4 whole 128-byte dW lines instead of 32 scattered 16-byte pieces
+        // (reads of tb are conflict-free: bank = nsub + 4 c4 + const)
+        const int c4 = lane & 7, nsub = lane >> 3;
+        if (a < P.n_atoms) {
+          int k = 0, ch = 0;
+          atom_elem(P, a, e_base + 4 * c4, k, ch);
+          if (k < A.kv && ((A.mask_filter >> k) & 1u)) {
 #pragma unroll
-          for (int qq = 0; qq < 8; ++qq) {
-            int k = 0, ch = 0;
-            atom_elem(P, a, e_base + 4 * qq, k, ch);
-            if (k < A.kv && ((A.mask_filter >> k) & 1u)) {
-              const float *src = tb + lane * 33 + 4 * qq;
-              red_add_v4(A.ws + (static_cast<int64_t>(n) * A.kv + k) * A.C + ch, src[0], src[1], src[2],
-                         src[3]);
+            for (int cc = 0; cc < 8; ++cc) {
+              const int col = cc * 4 + nsub;
+              const int n = n0 + col;
+              if (n < A.K) {
+                const float *src = tb + col * 33 + 4 * c4;
+                red_add_v4(A.ws + (static_cast<int64_t>(n) * A.kv + k) * A.C + ch, src[0], src[1], src[2],
+                           src[3]);
+              }
             }
           }
         }
