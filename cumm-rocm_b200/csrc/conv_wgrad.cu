@@ -62,6 +62,9 @@ struct WMeta {
   uint32_t active_bits;  // bit j -> M-tile t0 + j active for this chunk
   uint32_t grp[4];
 };
+__host__ __device__ constexpr uint32_t kScratchOff(int tab_f) {
+  return static_cast<uint32_t>(((tab_f * kRows + kRows) * 4 + sizeof(WMeta) + 15) & ~15u);
+}
 
 struct WParams {
   CUtensorMap tmap_in;    // input rows [in_rows, C], one-row boxes (gather path)
@@ -393,8 +396,127 @@ __global__ void __maxnreg__(kPair ? 80 : 96) conv_wgrad_kernel(const __grid_cons
     const int t = threadIdx.x - kLoadWarp0 * 32;
     const int r = t & 63;                  // row of the chunk
     const int par = kPair ? 0 : (t >> 6);  // filter parity of this thread (single layout)
+    bool async_done = false;
+    if constexpr (kPair) {
+      if (A.idx_sorted != nullptr) {
+        // Asynchronous form (pair layout, sorted index table).  The argsort
+        // entry, the two mask words and the group's index values of this
+        // thread's row are cp.async copies into the chunk's index buffer,
+        // issued kAhead chunks before the chunk is gated and published, so
+        // the memory round trips of consecutive chunks overlap.  A thread
+        // copies and then gates only its own row's values, so
+        // cp.async.wait_group alone orders them; the idx_full arrival
+        // publishes the gated table.  Two of the four buffers in flight as
+        // copies leave two published ahead of the producers (three in flight
+        // left too few published and was slower).
+        constexpr int kAhead = 2;
+        static_assert(kAhead < kIdxStages, "a buffer is refilled only after its chunk is published");
+        const uint32_t scr_off = kScratchOff(kTabF);
+        // copies of iteration j into buffer j % kIdxStages (an empty commit
+        // group past the last chunk); false when the buffer wait ran out
+        auto issue = [&](int j) -> bool {
+          const int64_t c = static_cast<int64_t>(c_begin) + static_cast<int64_t>(j) * c_step;
+          if (c < c_end) {
+            const int b = j % kIdxStages;
+            const uint32_t ph = (j / kIdxStages) & 1;
+            if (!mbar_wait(&idx_empty[b], ph ^ 1, abort_flag)) {
+              cp_async_commit();
+              return false;
+            }
+            const uint32_t base = smem_u32(smem + P.idx_off + b * P.idx_buf_bytes);
+            const int64_t row = c * kRows + r;
+            const int64_t row2 = c * kRows + (r ^ 32);
+            const bool valid = row < A.N;
+            if (A.argsort)
+              cp_async_4(base + (kTabF * kRows + r) * 4, A.argsort + (valid ? row : 0), valid ? 4u : 0u);
+            if (A.mask) {
+              int64_t wi = P.mw_shift >= 0 ? row >> P.mw_shift : row / A.mask_width;
+              bool ok1 = valid && wi < A.mask_count;
+              cp_async_4(base + scr_off + r * 4, A.mask + (ok1 ? wi : 0), ok1 ? 4u : 0u);
+              wi = P.mw_shift >= 0 ? row2 >> P.mw_shift : row2 / A.mask_width;
+              ok1 = row2 < A.N && wi < A.mask_count;
+              cp_async_4(base + scr_off + (kRows + r) * 4, A.mask + (ok1 ? wi : 0), ok1 ? 4u : 0u);
+            }
+#pragma unroll
+            for (int q = 0; q < kNQ; ++q) {
+              const int k = k_lo + q;
+              if (k < k_hi)
+                cp_async_4(base + ((k - k_lo) * kRows + r) * 4,
+                           A.idx_sorted + (valid ? static_cast<int64_t>(k) * A.N + row : 0), valid ? 4u : 0u);
+            }
+          }
+          cp_async_commit();
+          return true;
+        };
+        bool ok = true;
+#pragma unroll 1
+        for (int j = 0; j < kAhead && ok; ++j) ok = issue(j);
+#pragma unroll 1
+        for (int it = 0; ok; ++it) {
+          const int64_t c = static_cast<int64_t>(c_begin) + static_cast<int64_t>(it) * c_step;
+          if (c >= c_end) break;
+          cp_async_wait<kAhead - 1>();  // this thread's copies of iteration it have landed
+          const int b = it % kIdxStages;
+          uint8_t *buf = smem + P.idx_off + b * P.idx_buf_bytes;
+          int *tab = reinterpret_cast<int *>(buf);
+          int *sig_tab = tab + kTabF * kRows;
+          WMeta *meta = reinterpret_cast<WMeta *>(sig_tab + kRows);
+          const uint32_t *scr = reinterpret_cast<const uint32_t *>(buf + scr_off);
+          const int64_t row = c * kRows + r;
+          const int64_t row2 = c * kRows + (r ^ 32);
+          const bool valid = row < A.N;
+          int sig = valid ? (A.argsort ? sig_tab[r] : static_cast<int>(row)) : -1;
+          uint32_t word, w_other;
+          if (A.mask) {
+            word = scr[r];
+            w_other = scr[kRows + r];
+          } else {
+            word = valid ? 0xffffffffu : 0u;
+            w_other = row2 < A.N ? 0xffffffffu : 0u;
+          }
+          if (valid && (sig < 0 || sig >= A.dout_rows)) {
+            flag_error(A.err, kErrBadIndex);
+            sig = -1;
+          }
+          word &= A.mask_filter;
+          w_other &= A.mask_filter;
+          uint32_t cm = word | w_other;
+#pragma unroll
+          for (int s = 16; s > 0; s >>= 1) cm |= __shfl_xor_sync(0xffffffffu, cm, s);
+          sig_tab[r] = sig;
+#pragma unroll
+          for (int q = 0; q < kNQ; ++q) {
+            const int k = k_lo + q;
+            if (k < k_hi) {
+              int v = tab[q * kRows + r];
+              v = (((word >> k) & 1u) && sig >= 0) ? v : -1;
+              if (v < -1 || v >= A.in_rows) {
+                flag_error(A.err, kErrBadIndex);
+                v = -1;
+              }
+              tab[q * kRows + r] = v;
+            }
+          }
+          if (t < 32) {
+            const bool on = lane < t1 - t0 && (tile_fbits[lane] & cm) != 0;
+            const uint32_t bits = __ballot_sync(0xffffffffu, on);
+            if (t == 0) {
+              meta->active_bits = bits;
+              meta->n_active = __popc(bits);
+            }
+          }
+          mbar_arrive(&idx_full[b]);
+          if (!issue(it + kAhead)) ok = false;
+        }
+        cp_async_wait_all();
+        if (!ok) flag_error(A.err, kErrWaitTimeout);
+        async_done = true;
+      }
+    }
+    // synchronous form (single layout, or no sorted table): every load of a
+    // chunk is issued before any result is used
     int it = 0;
-    for (int c = c_begin; c < c_end; c += c_step, ++it) {
+    for (int c = async_done ? c_end : c_begin; c < c_end; c += c_step, ++it) {
       const int b = it % kIdxStages;
       const uint32_t ph = (it / kIdxStages) & 1;
       if (!mbar_wait(&idx_empty[b], ph ^ 1, abort_flag)) {
@@ -770,7 +892,7 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs &a, int num_sms, cudaStream_t 
   const uint32_t bar_bytes = 512;
   auto idx_buf_for = [](bool pr) {
     const int f = pr ? Layout<true>::kTabF : Layout<false>::kTabF;
-    return static_cast<uint32_t>(((f * kRows + kRows) * 4 + sizeof(WMeta) + 127) & ~size_t(127));
+    return static_cast<uint32_t>((kScratchOff(f) + 2 * kRows * 4 + 127) & ~size_t(127));
   };
   // stages that fit beside the index ring, barriers and dOut buffers in one
   // CTA's dynamic shared memory: 227 KB alone on an SM, 113 KB for one of two

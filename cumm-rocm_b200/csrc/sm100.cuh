@@ -83,6 +83,11 @@ __device__ __forceinline__ void cp_async_16(uint32_t dst, const void *src, uint3
                "r"(src_bytes)
                : "memory");
 }
+// 4-byte global->shared copy (L1-allocating); src_bytes == 0 zero-fills.
+__device__ __forceinline__ void cp_async_4(uint32_t dst, const void *src, uint32_t src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(src_bytes)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
