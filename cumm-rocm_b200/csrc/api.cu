@@ -113,15 +113,41 @@ struct ConvPlan {
   int64_t ws_min = 0;    // what a call cannot run without
 };
 
-// Workspace head of the tcgen05 forward / backward-input kernels (zeroed per
-// call): the tile counter of their dynamic scheduler, then the histogram and
-// block counter of the largest-first tile order.  The per-tile offset counts
-// and the order itself follow, ceil(N / 128) ints each.
+// Workspace of the tcgen05 forward / backward-input kernels: a 256-byte head
+// (the tile counter of the row-gather kernel's dynamic scheduler, zeroed per
+// call), for backward-input without an MN-major weight the transposed
+// [C, kv, K] weight, and, when the caller gives no indices_sorted and the
+// strand kernel can take the layer, the index table permuted into argsort
+// order (kv x N int32) that this call writes itself.
 constexpr int64_t kSchedBytes = 256;
 
-int64_t sched_bytes(int64_t N) {
-  const int64_t m_tiles = (N + 127) / 128;
-  return kSchedBytes + 2 * align256(m_tiles * 4);
+// Output-column tile of the tcgen05 forward / backward-input kernels.
+int64_t column_tile(int64_t ncols, int32_t tile_n) {
+  if (tile_n > 0) return tile_n;
+  int64_t bn = ncols;
+  int tiles = 1;
+  while (bn > 256 || bn % 16) {
+    ++tiles;
+    while (ncols % tiles || (ncols / tiles) % 16) ++tiles;
+    bn = ncols / tiles;
+  }
+  return bn;
+}
+
+// Bytes of the sorted index table a forward / backward-input call builds for
+// the strand kernel when the caller passes none (0 when the strand kernel
+// would not take the layer: rows of 64 bytes or whole 128-byte blocks,
+// column tile <= 64, N % 4 == 0).  Building it costs one gather of kv x N
+// ints; the strand kernel then runs ~2x faster than the row-gather kernel
+// reading the unsorted table through the argsort.
+int64_t own_sorted_bytes(const sc_conv_params *p, int es) {
+  if (p->indices_sorted != nullptr || p->N <= 0 || p->N % 4 != 0) return 0;
+  const bool fwd = p->op_type == SC_CONV_FORWARD;
+  const int64_t rb = (fwd ? p->C : p->K) * es;
+  const int64_t ncols = fwd ? p->K : p->C;
+  if (!((rb == 64 && p->kv > 1) || (rb >= 128 && rb % 128 == 0))) return 0;
+  if (column_tile(ncols, p->tile_n) > 64) return 0;
+  return align256(static_cast<int64_t>(p->kv) * p->N * 4);
 }
 
 int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
@@ -213,7 +239,8 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
       return fail(SC_RUNTIME, "Can't Found Algorithm: C=%lld K=%lld not tiled by the tcgen05 kernel "
                   "(C*sizeof in {16,32,64} or a multiple of 16 >= 128 bytes; K %% 16 == 0)",
                   (long long)p->C, (long long)p->K);
-    plan->ws_bytes = sched_bytes(p->N);  // optional: without it tiles are dealt statically
+    // optional: without it tiles are dealt statically and the unsorted table is read
+    plan->ws_bytes = kSchedBytes + own_sorted_bytes(p, esize(di));
     return SC_OK;
   }
   if (op == SC_CONV_BACKWARD_INPUT) {
@@ -223,8 +250,8 @@ int plan_conv(const sc_conv_params *p, ConvPlan *plan) {
     if (!rowgather_width_ok(p->K * esize(di)) || p->C % 16)
       return fail(SC_RUNTIME, "Can't Found Algorithm: K=%lld C=%lld not tiled by the tcgen05 kernel",
                   (long long)p->K, (long long)p->C);
-    plan->ws_bytes = sched_bytes(p->N) + align256(p->K * p->kv * p->C * esize(di));
-    plan->ws_min = plan->ws_bytes;
+    plan->ws_min = kSchedBytes + align256(p->K * p->kv * p->C * esize(di));
+    plan->ws_bytes = plan->ws_min + own_sorted_bytes(p, esize(di));
     return SC_OK;
   }
   // backward weight
@@ -382,15 +409,10 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     const int64_t ncols = fwd ? p->K : p->C;  // output columns
     scb::ConvRowGatherArgs a{};
     uint8_t *ws = static_cast<uint8_t *>(p->workspace);
-    // schedule state in the workspace head (zeroed by the launcher); the
-    // largest-first order is the caller's when given, else computed here
-    if (ws != nullptr && p->workspace_bytes >= plan.ws_bytes) {
-      const int64_t order_bytes = align256((p->N + 127) / 128 * 4);
-      a.tile_counter = reinterpret_cast<int *>(ws);
-      a.sched_head = reinterpret_cast<int *>(ws) + 1;
-      a.tile_pc = reinterpret_cast<int32_t *>(ws + kSchedBytes);
-      a.tile_order = reinterpret_cast<int32_t *>(ws + kSchedBytes + order_bytes);
-    }
+    // the tile counter in the workspace head (zeroed by the launcher); a
+    // largest-first order only when the caller gives one (computing it per
+    // call costs about what it saves)
+    if (ws != nullptr && p->workspace_bytes >= kSchedBytes) a.tile_counter = reinterpret_cast<int *>(ws);
     if (p->tile_order != nullptr) {
       a.tile_order = p->tile_order;
       a.order_given = 1;
@@ -399,18 +421,8 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     a.a_rows = fwd ? p->n_in : p->n_out;
     a.a_row_bytes = static_cast<int>(red * es);
     a.a_row_stride = red * es;
-    int tiles = 1;
-    int64_t bn = ncols;
-    if (p->tile_n > 0) {
-      bn = p->tile_n;
-      tiles = static_cast<int>(ncols / bn);
-    } else {
-      while (bn > 256 || bn % 16) {
-        ++tiles;
-        while (ncols % tiles || (ncols / tiles) % 16) ++tiles;
-        bn = ncols / tiles;
-      }
-    }
+    const int64_t bn = column_tile(ncols, p->tile_n);
+    const int tiles = static_cast<int>(ncols / bn);
     // backward-input reads the weight MN-major when the slabs are whole
     // 64 x 64 boxes of 16-bit data, else from a transposed [C, kv, K] copy
     const bool b_mn = !fwd && es == 2 && red % 64 == 0 && bn % 64 == 0 && p->n_out > 0 &&
@@ -418,10 +430,10 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     if (fwd || b_mn) {
       a.b_base = static_cast<const uint8_t *>(p->weight);
     } else {
-      e = scb::launch_transpose_weight(p->weight, ws + sched_bytes(p->N), static_cast<int>(p->K), p->kv,
+      e = scb::launch_transpose_weight(p->weight, ws + kSchedBytes, static_cast<int>(p->K), p->kv,
                                        static_cast<int>(p->C), es, s);
       if (e != cudaSuccess) return cuda_fail(e, "weight transpose launch");
-      a.b_base = ws + sched_bytes(p->N);
+      a.b_base = ws + kSchedBytes;
     }
     a.b_mn = b_mn ? 1 : 0;
     // B rows: [n, kv, red] (K-major), or for b_mn the weight's [red, kv, n]
@@ -437,6 +449,15 @@ int sc_conv_implicit_gemm(const sc_conv_params *p) {
     a.indices = p->indices;
     a.a_inds = nullptr;
     a.idx_sorted = p->indices_sorted;
+    // no sorted table given: build one at the end of the workspace when the
+    // strand kernel can take the layer (results are the same either way)
+    const int64_t own = own_sorted_bytes(p, es);
+    if (own > 0 && ws != nullptr && p->workspace_bytes >= plan.ws_bytes) {
+      int32_t *tab = reinterpret_cast<int32_t *>(ws + plan.ws_bytes - own);
+      e = scb::sort_indices(p->indices, p->kv, p->N, p->mask_argsort, tab, s);
+      if (e != cudaSuccess) return cuda_fail(e, "sorted index table");
+      a.idx_sorted = tab;
+    }
     a.mask_out = fwd ? p->mask_output : nullptr;
     a.tile_m_desp = p->tile_m;
     a.mask_filter = p->mask_filter;

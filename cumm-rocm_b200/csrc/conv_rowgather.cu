@@ -1443,22 +1443,10 @@ cudaError_t launch_tile_order(const uint32_t *mask, int64_t M, uint32_t filter, 
 }
 
 namespace {
-// Zeroes the schedule head (tile counter and histogram) and, unless the
-// caller gave an order, writes the largest-first order.
+// Zeroes the row-gather kernel's tile counter (the strand kernel has none).
 cudaError_t prepare_schedule(const ConvRowGatherArgs &a, bool counter, cudaStream_t stream) {
-  if (a.order_given) {
-    if (!counter || a.tile_counter == nullptr) return cudaSuccess;
-    return cudaMemsetAsync(a.tile_counter, 0, sizeof(int), stream);
-  }
-  if (a.tile_order == nullptr) {
-    if (!counter || a.tile_counter == nullptr) return cudaSuccess;
-    return cudaMemsetAsync(a.tile_counter, 0, sizeof(int), stream);
-  }
-  // the head is the tile counter followed by the 34 ints of sched_head
-  cudaError_t e = cudaMemsetAsync(a.tile_counter, 0, 35 * sizeof(int), stream);
-  if (e != cudaSuccess) return e;
-  return launch_tile_order(a.mask, a.M, a.mask_filter, a.reverse, a.kv, a.sched_head, a.tile_pc,
-                           const_cast<int32_t *>(a.tile_order), stream);
+  if (!counter || a.tile_counter == nullptr) return cudaSuccess;
+  return cudaMemsetAsync(a.tile_counter, 0, sizeof(int), stream);
 }
 }  // namespace
 

@@ -64,13 +64,9 @@ struct ConvRowGatherArgs {
   int64_t out_rows;          // bound for output rows
   const int32_t *idx_sorted; // optional [kv, M]: indices[k][argsort[r]]
   int *tile_counter;         // optional, zero at launch: tiles handed out dynamically
-  // optional largest-first tile schedule: tile_order holds ceil(M / 128)
-  // ints.  With order_given it was computed by the caller; otherwise the
-  // launcher computes it first, using sched_head (34 ints: 33 histogram bins
-  // and a block counter, zeroed by the launcher) and tile_pc (ceil(M / 128)
-  // ints).  tile_counter, when set, is zeroed by the launcher as well.
-  int *sched_head;
-  int32_t *tile_pc;
+  // optional largest-first tile schedule given by the caller (order_given
+  // set): ceil(M / 128) ints, a permutation of the row tiles.  tile_counter,
+  // when set, is zeroed by the launcher.
   const int32_t *tile_order;
   int order_given;
   int m_tiles;               // ceil(M / 128), set by the launcher

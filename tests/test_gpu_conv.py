@@ -516,12 +516,12 @@ def test_strand_kernel_fp8_and_bad_index():
 
 @pytest.mark.parametrize("use_sorted", [True, False])
 def test_tile_schedule_does_not_change_results(use_sorted):
-    """With a workspace the forward hands its 128-row tiles out heaviest
-    first (a per-call counting sort of the tiles by the offsets they visit);
-    without one (a workspace is optional for the forward) it deals them in
-    mask order.  Each tile is computed by one pipeline alone, so both give
-    bit-identical outputs and mask_output, on the strand kernel (sorted index
-    table) and on the row-gather kernel, and match the FP64 oracle."""
+    """With a tile order (PairTable.tile_order) the forward hands its 128-row
+    tiles out heaviest first; without one it deals them in mask order, and
+    without a workspace (optional for the forward) it also reads the unsorted
+    index table on the row-gather kernel.  Each tile is computed by one
+    pipeline alone, so all give bit-identical outputs and mask_output, and
+    match the FP64 oracle."""
     import ctypes
     from cumm import _lib
     from cumm.conv.main import ConvMainUnitTest, build_conv_params_c
@@ -649,9 +649,8 @@ def test_strand_kernel_e4m3_64byte_rows(n, K, tile_m):
 def test_tile_order_backward_input_and_split_masks():
     """The largest-first order made for the forward masks serves the
     submanifold backward-input (reverse_mask) and each mask split of the
-    MaskSplitImplicitGemm form: results are bit-identical to calls that get a
-    workspace but no order (each computes the order itself) and match the FP64
-    oracle."""
+    MaskSplitImplicitGemm form: results are bit-identical to calls without an
+    order (tiles in mask order) and match the FP64 oracle."""
     import ctypes
     from cumm import _lib
     from cumm.conv.main import ConvMainUnitTest, build_conv_params_c
@@ -722,3 +721,49 @@ def test_tile_order_backward_input_and_split_masks():
     # one-launch tolerance; the forward accumulates into fp32
     _assert_close(dins[0].double().numpy(), co.dgrad_gather_gemm_scatter(to64(dy), to64(w), pb), 2 * TOL_16)
     _assert_close(outs[0].double().numpy(), co.fwd_gather_gemm_scatter(to64(x), to64(w), pf), TOL_16)
+
+
+
+def test_default_path_builds_sorted_table():
+    """A call without indices_sorted builds the sorted index table in its
+    workspace and runs the strand kernel: bit-identical to the call given the
+    table.  With a workspace too small for the table (the forward's is
+    optional) it reads the unsorted table on the row-gather kernel, equal up to
+    fp32 summation order."""
+    import ctypes
+    from cumm import _lib
+    from cumm.conv.main import ConvMainUnitTest, build_conv_params_c
+    from cumm.spconv_ops import build_pair_table
+    from cumm.tensorview.gemm import ConvParams
+    n, C, K = 30000, 64, 64
+    coords = vg.lidar_voxels(n, seed=17)
+    pt = build_pair_table(torch.from_numpy(coords).cuda(), vg.KITTI_SHAPE)
+    rng = np.random.default_rng(17)
+    x = dev(rng.standard_normal((n, C)).astype(np.float32), torch.bfloat16)
+    w = dev(vg.kaiming_uniform(K, 27, C, 17), torch.bfloat16)
+    outs = []
+    for mode in ("given", "default", "small_ws"):
+        p = ConvParams(3, ConvOpType.kForward)
+        p.conv_algo_desp = find_desp(ConvOpType.kForward, "Tcgen05", tv.bfloat16, tv.bfloat16, tv.float32, 128)
+        o = torch.full((n, K), float("nan"), dtype=torch.float32, device="cuda")
+        p.input, p.weight, p.output = tv.Tensor(x), tv.Tensor(w), tv.Tensor(o)
+        p.indices = tv.Tensor(pt.pairs_fwd)
+        p.mask = tv.Tensor(pt.masks_fwd[0], tv.uint32)
+        p.mask_argsort = tv.Tensor(pt.argsorts_fwd[0])
+        if mode == "given":
+            p.indices_sorted = tv.Tensor(pt.sorted_indices("fwd"))
+        if mode != "small_ws":
+            ConvMainUnitTest(sync_check=True).implicit_gemm2(p)
+        else:
+            cp, _info = build_conv_params_c(p)
+            cp.flags |= _lib.SC_FLAG_SYNC_CHECK
+            ws = torch.empty(256, dtype=torch.uint8, device="cuda")
+            cp.workspace, cp.workspace_bytes = ws.data_ptr(), 256
+            _lib.check(_lib.load().sc_conv_implicit_gemm(ctypes.byref(cp)))
+        torch.cuda.synchronize()
+        outs.append(o.cpu())
+    assert torch.equal(outs[0], outs[1])
+    nr = ((outs[2] - outs[0]).norm() / outs[0].norm()).item()
+    assert nr < 1e-6, nr
+    ref = co.fwd_gather_gemm_scatter(to64(x), to64(w), pt.pairs_fwd.cpu().numpy())
+    _assert_close(outs[0].double().numpy(), ref, TOL_16)

@@ -58,13 +58,17 @@ def _ws(cp):
 
 
 def test_conv_validation_codes():
-    # fwd: tile counter and largest-first schedule (optional): a 256-byte head,
-    # then ceil(N / 128) per-tile offset counts and the tile order, each
-    # rounded up to 256 bytes (N = 1000: 8 tiles)
-    sched = 256 + 2 * 256
-    assert _ws(_fake_conv())[:2] == (0, sched)
+    # fwd (optional workspace): the tile counter head, then the sorted index
+    # table the call builds for the strand kernel when none is given
+    # (kv x N int32, rounded up to 256 bytes)
+    own = ((27 * 1000 * 4 + 255) // 256) * 256
+    assert _ws(_fake_conv())[:2] == (0, 256 + own)
     rc, n, _ = _ws(_fake_conv(1))
-    assert rc == 0 and n == sched + 64 * 27 * 64 * 2  # dgrad: schedule + transposed weight
+    assert rc == 0 and n == 256 + 64 * 27 * 64 * 2 + own  # dgrad: + transposed weight
+    # with indices_sorted given, or a layer the strand kernel does not take
+    # (N % 4 != 0), no table is built
+    assert _ws(_fake_conv(indices_sorted=0x3000))[:2] == (0, 256)
+    assert _ws(_fake_conv(N=1001, n_in=1001, n_out=1001, mask_count=1001))[:2] == (0, 256)
     rc, n, _ = _ws(_fake_conv(2))
     assert rc == 0 and n == 64 * 27 * 64 * 4          # wgrad: fp32 accumulation
     rc, _, msg = _ws(_fake_conv(0, N=999))
