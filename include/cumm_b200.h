@@ -124,7 +124,10 @@ typedef struct sc_conv_params {
    * indices_sorted[k][r] = indices[k][mask_argsort[r]] ([kv, N] int32), as
    * produced by sc_sort_indices.  With it the kernels read the index table
    * coalesced instead of through the argsort indirection; results are
-   * identical. */
+   * identical.  Without it, a forward / backward-input call whose layer the
+   * strand kernel takes builds the table at the end of its workspace (the
+   * size sc_conv_workspace_size reports includes it); pass it when a pair
+   * table serves several calls. */
   const int32_t *indices_sorted;
   /* Output-column tile of the tcgen05 forward / backward-input kernels (the
    * reference's ConvAlgoDesp tile_shape[1]): 0 picks the widest tile (all
@@ -134,10 +137,9 @@ typedef struct sc_conv_params {
   /* Optional (may be NULL): the order in which the tcgen05 forward /
    * backward-input kernels take their 128-row tiles, ceil(N / 128) int32
    * entries, a permutation of 0 .. ceil(N / 128) - 1 as sc_tile_order writes
-   * it.  Results do not depend on it.  Without it (and with a workspace) each
-   * call computes the order itself, which costs a small kernel per call; an
-   * entry outside the range sets error bit 1 and its tile is skipped (the
-   * permutation property itself is not checked). */
+   * it.  Results do not depend on it.  Without it the tiles are taken in
+   * mask order.  An entry outside the range sets error bit 1 and its tile is
+   * skipped (the permutation property itself is not checked). */
   const int32_t *tile_order;
 } sc_conv_params;
 
