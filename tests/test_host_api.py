@@ -197,3 +197,22 @@ def test_misaligned_tile_order_rejected():
     rc, _, msg = _ws(_fake_conv(0, tile_order=0x1002))
     assert rc == _lib.SC_INVALID_ARG and "tile_order" in msg
     assert _ws(_fake_conv(0, tile_order=0x1004))[0] == 0
+
+
+def test_own_sorted_table_predicate():
+    """The workspace a forward reports includes the sorted index table it
+    builds for the strand kernel exactly when that kernel takes the layer:
+    64-byte rows or whole 128-byte blocks, a column tile <= 64 and N % 4 == 0."""
+    own = ((27 * 1000 * 4 + 255) // 256) * 256
+    cases = [
+        (dict(C=32), True),                      # 64-byte rows
+        (dict(C=128), True),                     # two 128-byte blocks per offset
+        (dict(C=16), False),                     # 32-byte rows: packed row-gather path
+        (dict(K=128), False),                    # widest column tile 128
+        (dict(K=128, tile_n=64), True),          # column tile 64
+        (dict(C=96), False),                     # 192-byte rows
+    ]
+    for kw, builds in cases:
+        rc, n, msg = _ws(_fake_conv(0, **kw))
+        assert rc == 0, (kw, msg)
+        assert n == 256 + (own if builds else 0), (kw, n)
